@@ -1,0 +1,315 @@
+"""Benchmark: plain elastic P/S RTM shots on B200 (one JSON line on rank 0).
+
+Workload (the headline metric's configuration): 1000 x 500 interior,
+dx = 5 m, 30-cell CPML (1060 x 560 padded), 10th-order (N = 5) staggered
+stencil, dt = 0.5 ms, nt = 4000, 25 Hz Ricker; 8 seeded flat layers,
+migration model Gaussian-smoothed (sigma = 10 cells); 40 shot positions on
+z = 2 with full-spread receivers.  Observed records are modelled once with
+the true model before timing (acquisition, not migration).
+
+One step = one RTM shot: forward with boundary-strip save, receiver
+back-propagation with record injection, source-wavefield reconstruction,
+PP/PS imaging, image normalisation + Laplacian and the FP64 stack.
+
+  value : Gcell-updates/s with records resident in HBM (device API)
+  e2e   : the same through ouc_rtm_shot with pinned host buffers (records
+          in, images out, copies inside the timed region)
+  N > 1 : one process per GPU, shots sharded round-robin, FP64 stacks
+          all-reduced once at the end (weak scaling)
+
+--impl reference times the CPU transcription of the reference kernels
+(OpenMP, float) on the same grid for a bounded number of time steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s & RTM shots/hr on 1 B200, learned vs plain at <=1% L2 vs FP64"
+UNIT = "Gcell-updates/s"
+
+
+def algorithmic_bytes_forward(cfg, n_rcv, ring_cells, strip_bytes_per_value=4):
+    """Algorithmic HBM bytes of one forward step (each byte moved once):
+    56 B per cell (read P/S at levels n and n-1, Vp^2 and Vs^2, write level
+    n+1), 48 B per damped cell per axis (six CPML memories read + written),
+    8 B per receiver, and the boundary ring of 8 fields written."""
+    X, Z, L = cfg.X, cfg.Z, cfg.npml
+    C = X * Z
+    c_xpml = (2 * L - 1) * Z
+    c_zpml = (2 * L - 1) * X
+    return 56 * C + 48 * (c_xpml + c_zpml) + 8 * n_rcv + 8 * ring_cells * strip_bytes_per_value
+
+
+def ring_cells(cfg):
+    N = cfg.half_order
+    return 4 * N * (cfg.nx + cfg.nz)
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while alive."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    p = os.path.join(ROOT, "profiles", "k_step_fwd_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_sample(steps_hint=None, threads=None, budget_s=12.0):
+    """FP32 OpenMP transcription of the reference kernels (oracle) on the
+    benchmark grid: one RTM shot truncated to a bounded number of time steps.
+    Returns (Gcell-updates/s, cores, sample description)."""
+    from oracle.oracle import Oracle, Shot
+    from ouc_b200 import models
+    orc = Oracle()
+    cores = orc.threads(threads or os.cpu_count())
+    w = models.c2()
+    cfg = w.cfg
+    X, Z, L = cfg.X, cfg.Z, cfg.npml
+    vp = orc.pad(np.pad(w.vp_mig, L), L)
+    vs = orc.pad(np.pad(w.vs_mig, L), L)
+    ax, az = orc.profile(vp, L)
+    from ouc_b200 import ricker
+    nts = steps_hint or 8
+    while True:
+        src, t0 = ricker(w.fm, cfg.dt, nts)
+        sh = Shot(X=X, Z=Z, L=L, N=cfg.half_order, nt=nts, sx=L + w.shots[0].sx, sz=L + 2, rz=L + 2, dx=cfg.dx,
+                  dz=cfg.dz, dt=cfg.dt, t0=t0)
+        t1 = time.perf_counter()
+        orc.rtm(sh, vp, vs, ax, az, src)
+        el = time.perf_counter() - t1
+        if steps_hint or el > budget_s / 4 or nts >= 4000:
+            break
+        nts = min(4000, int(nts * max(2.0, budget_s / max(el, 1e-3) * 0.9)))
+    cells = nts * (2 * X * Z + cfg.nx * cfg.nz)
+    return cells / el / 1e9, cores, f"one RTM shot of the benchmark grid truncated to nt={nts} steps ({el:.1f} s)"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    vals = []
+    desc = None
+    cores = None
+    for _ in range(args.warmup):
+        cpu_sample(steps_hint=8)
+    for _ in range(args.steps):
+        v, cores, desc = cpu_sample(steps_hint=args.ref_steps)
+        vals.append(v)
+    value = statistics.median(vals)
+    from ouc_b200 import models
+    w = models.c2()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "grid": [w.cfg.X, w.cfg.Z], "nt": w.cfg.nt, "half_order": w.cfg.half_order},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ouc", choices=["ouc", "reference"])
+    ap.add_argument("--nt", type=int, default=4000, help="time steps per shot (the workload's 4000)")
+    ap.add_argument("--ref-steps", type=int, default=None, help="CPU sample length (time steps)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    import ouc_b200 as o
+    from ouc_b200 import models
+    w = models.c2(nt=args.nt)
+    cfg = w.cfg
+    cfg.device = local
+    wavelet, t0 = o.ricker(w.fm, cfg.dt, cfg.nt)
+    X, nt = cfg.X, cfg.nt
+
+    # observed records with the true model (not timed), a few shot positions reused
+    nrec_shots = min(4, len(w.shots))
+    my_shots = [w.shots[(rank + k * world) % len(w.shots)] for k in range(nrec_shots)]
+    for s in my_shots:
+        s.t0 = t0
+    true_ctx = o.Context(cfg, w.vp, w.vs, w.rho)
+    records = [true_ctx.forward(s, wavelet)[:2] for s in my_shots]
+    true_ctx.close()
+    mig = o.Context(cfg, w.vp_mig, w.vs_mig, w.rho)
+    stream = torch.cuda.ExternalStream(mig.stream, device=torch.device("cuda", local))
+
+    # device-resident inputs
+    d_w = torch.from_numpy(wavelet).cuda()
+    d_rec = [(torch.from_numpy(r[0]).cuda(), torch.from_numpy(r[1]).cuda()) for r in records]
+    d_img = torch.empty((2, cfg.nx, cfg.nz), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MiB > L2
+    torch.cuda.synchronize()
+
+    def shot_dev(k):
+        s = my_shots[k % nrec_shots]
+        rx, rz = d_rec[k % nrec_shots]
+        mig.rtm_shot_dev(s, d_w.data_ptr(), rx.data_ptr(), rz.data_ptr(), d_img[0].data_ptr(), d_img[1].data_ptr())
+
+    for k in range(args.warmup):
+        shot_dev(k)
+    launches_per_shot = mig.timing()["kernel_launches"]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    fwd_ms = []
+    bwd_ms = []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))          # between timed shots: evict L2
+            ev[k][0].record(stream)
+        shot_dev(k)                        # synchronous on the context stream
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+        t = mig.timing()
+        fwd_ms.append(t["forward_ms"])
+        bwd_ms.append(t["backward_ms"])
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        stk = torch.zeros(3 * cfg.nx * cfg.nz, dtype=torch.float64, device="cuda")
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.all_reduce(stk)   # the cross-shot FP64 stack exchange
+        dist.barrier()
+    clk = clocks.stop()
+    cells = w.cell_updates_per_shot()
+    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    shots_per_hour = 3600.0 * args.steps * world / (ms / 1e3)
+
+    # e2e through the host API with pinned buffers
+    pin = [(torch.from_numpy(r[0]).pin_memory().numpy(), torch.from_numpy(r[1]).pin_memory().numpy()) for r in records]
+    e2e_steps = max(2, args.steps // 2)
+    mig.rtm_shot(my_shots[0], wavelet, rec=pin[0])
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for k in range(e2e_steps):
+        mig.rtm_shot(my_shots[k % nrec_shots], wavelet, rec=pin[k % nrec_shots])
+    e2e_s = time.perf_counter() - t1
+    if world > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = cells * e2e_steps * world / e2e_s / 1e9
+
+    # roofline of the dominant kernel: the fused forward step (k_step, forward mode)
+    peak, peak_kind = measured_peak()
+    per_launch_ms = statistics.median(fwd_ms) / nt
+    abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg))
+    achieved = abytes / (per_launch_ms / 1e3) / 1e9
+    tr = committed_traffic()
+    traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name else None
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            v, cores, desc = cpu_sample()
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model, modelled records)",
+            "config": {"workload": w.name, "grid": [cfg.X, cfg.Z], "interior": [cfg.nx, cfg.nz], "nt": nt,
+                       "half_order": cfg.half_order, "dx_m": cfg.dx, "dt_s": cfg.dt, "step": "one RTM shot",
+                       "l2": "256 MiB buffer written between timed shots; 3.8 GB of boundary strips per shot",
+                       "parallelism": f"shots sharded over {world} GPU(s)"},
+            "shots_per_hour": shots_per_hour,
+            "phase_ms": {"forward": statistics.median(fwd_ms), "backward": statistics.median(bwd_ms)},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * nt * X * 4 + nt * 4,
+                    "d2h_bytes_per_step": 2 * cfg.nx * cfg.nz * 4, "shots_per_hour": 3600.0 * e2e_steps * world / e2e_s},
+            "roofline": {"kernel": "k_step<5, forward> (fused S+U stage, CPML, strip save)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": abytes,
+                         "launch_ms": per_launch_ms, "traffic": traffic},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches_per_shot * args.steps),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    mig.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,158 @@
+/*
+ * ouc.h -- C ABI of the B200-native elastic P/S-decoupled finite-difference
+ * modeling and reverse-time-migration library (libouc.so).
+ *
+ * The reference (gm340/ouc, P-S-seperating.cu) has no library API: its
+ * interface is a set of __global__ kernels driven by a monolithic main().
+ * Each entry point below replaces one stage of that main(); the comment on
+ * each names the reference lines whose role it takes over.  "PS:n" means
+ * P-S-seperating.cu line n.
+ *
+ * Conventions
+ *   - Every call returns an int status: OUC_OK (0) or an OUC_E* code; no
+ *     exception or abort crosses the ABI.  ouc_last_error() gives the detail.
+ *   - Grids are x-major with z contiguous: element (i, j) of an nx x nz
+ *     array is a[i * nz + j] (the reference's i * Zn + j, PS:224).
+ *   - "Padded" coordinates include the absorbing layer of npml cells on
+ *     every side (X = nx + 2 npml, Z = nz + 2 npml); source and receiver
+ *     positions in ouc_shot are interior coordinates (padded - npml).
+ *   - The caller owns host buffers; the library owns device buffers.  The
+ *     *_dev entry points take device pointers instead and do no host copy.
+ *   - A context is not thread-safe; use one context per host thread.  All
+ *     work is queued on the context's stream.
+ */
+#ifndef OUC_H
+#define OUC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OUC_VERSION_MAJOR 0
+#define OUC_VERSION_MINOR 1
+
+enum {
+    OUC_OK = 0,
+    OUC_EINVAL = 1,      /* bad argument or configuration                      */
+    OUC_ECUDA = 2,       /* a CUDA runtime call failed                          */
+    OUC_ENOMEM = 3,      /* device allocation failed                            */
+    OUC_EUNSTABLE = 4,   /* CFL limit exceeded or non-finite wavefield          */
+    OUC_ESTATE = 5,      /* call out of order (e.g. stack before any shot)      */
+    OUC_ETIMEOUT = 6,    /* a bounded device wait ran out                       */
+    OUC_ENODEV = 7       /* no usable sm_100 device                             */
+};
+
+enum { OUC_MODEL_INTERIOR = 0, OUC_MODEL_PADDED = 1 };
+/* Which time level the Vx/Vz boundary strips are restored at during the
+ * source-wavefield reconstruction.  REFERENCE reproduces PS:2337 (one level
+ * late, as the reference does); EXACT restores the level the inverse
+ * leapfrog needs, which reconstructs the source field to round-off. */
+enum { OUC_STRIP_REFERENCE = 0, OUC_STRIP_EXACT = 1 };
+/* Which source level the imaging condition correlates at back-step t:
+ * REFERENCE = the level the reference uses (PS:964, PS:2361), EXACT = the
+ * level whose records were injected at that step. */
+enum { OUC_IMAGE_REFERENCE = 0, OUC_IMAGE_EXACT = 1 };
+enum { OUC_PREC_FP32 = 0, OUC_PREC_FP16 = 1, OUC_PREC_BF16 = 2 };
+/* Source mechanism: THETA adds the wavelet to the dilatation stress at the
+ * source cell (PS:331-338, PS:380); FORCE_Z adds dt^2 * wavelet to the
+ * vertical P displacement (an extension with no reference counterpart). */
+enum { OUC_SRC_THETA = 0, OUC_SRC_FORCE_Z = 1 };
+/* Gather layout at the host boundary: receiver-major [X][nt] as the
+ * reference's record arrays (PS:308), or time-major [nt][X]. */
+enum { OUC_GATHER_XT = 0, OUC_GATHER_TX = 1 };
+
+typedef struct ouc_config {
+    int nx, nz;             /* interior grid                                     */
+    int npml;               /* absorbing width L in cells (PS:15)                */
+    int half_order;         /* stencil half-width N: 2..6 (PS:16 uses 6)          */
+    float dx, dz, dt;       /* spacing (m) and time step (s)                     */
+    int nt;                 /* time steps per shot (PS:17)                       */
+    float pml_r;            /* target reflection R of the damping profile (PS:23) */
+    int model_layout;       /* OUC_MODEL_INTERIOR or OUC_MODEL_PADDED            */
+    int strip_level;        /* OUC_STRIP_*                                       */
+    int image_align;        /* OUC_IMAGE_*                                       */
+    int strip_precision;    /* OUC_PREC_*: storage of the boundary strips        */
+    int compensated_image;  /* 1: compensated-FP32 per-shot accumulators         */
+    int gather_layout;      /* OUC_GATHER_*                                      */
+    int device;             /* CUDA device ordinal                               */
+    void* stream;           /* cudaStream_t to run on, or NULL for a private one */
+} ouc_config;
+
+typedef struct ouc_shot {
+    int sx, sz;             /* source cell, interior coordinates                 */
+    int rz;                 /* receiver row, interior z (receivers span all X)   */
+    int src_type;           /* OUC_SRC_*                                         */
+    int t0;                 /* wavelet delay in samples, for the mute (PS:1955)  */
+    int mute;               /* 1: direct-wave mute before back-propagation       */
+} ouc_shot;
+
+typedef struct ouc_ctx ouc_ctx;
+
+/* Per-call device timings (CUDA events on the context stream), ms. */
+typedef struct ouc_timing {
+    float forward_ms;       /* forward time loop                                 */
+    float backward_ms;      /* backward time loop incl. imaging                  */
+    float finalize_ms;      /* image normalisation, Laplacian, stack             */
+    float copy_ms;          /* host<->device copies inside the call              */
+    long long kernel_launches;
+} ouc_timing;
+
+const char* ouc_strerror(int status);
+const char* ouc_last_error(const ouc_ctx* ctx);
+int ouc_version(void);
+
+/* Float32 staggered-grid weights a_1..a_N the library uses (PS:221 for N=6,
+ * the exact Taylor solution rounded to float32 otherwise). */
+int ouc_stencil_weights(int half_order, float* out);
+
+/* Ricker wavelet as built by main() (PS:1954-1958): out[nt], *t0 = delay. */
+int ouc_ricker(float fm, float dt, int nt, float* out, int* t0);
+
+/* Create a context: uploads the model, pads it into the absorbing layer
+ * (xiangbian, PS:37-119), builds the damping profile (PS:2067-2105) and
+ * allocates all device state.  vp/vs/rho are nx*nz (OUC_MODEL_INTERIOR) or
+ * X*Z (OUC_MODEL_PADDED); rho may be NULL and is not used by the
+ * reference's density-normalised equations (PS:373-378). */
+int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const float* rho, ouc_ctx** out);
+int ouc_destroy(ouc_ctx* ctx);
+int ouc_dims(const ouc_ctx* ctx, int* X, int* Z);
+void* ouc_stream(const ouc_ctx* ctx);
+int ouc_last_timing(const ouc_ctx* ctx, ouc_timing* t);
+/* Device bytes held by the context (state, strips, staging). */
+size_t ouc_device_bytes(const ouc_ctx* ctx);
+
+/* Forward modeling of one shot: the reference's forward time loop
+ * (forward_s + forward_u, PS:2258-2266) with receiver extraction (PS:307-311,
+ * post-update values).  gather_vx/vz: X*nt each in cfg->gather_layout, or
+ * NULL.  fields: optional 6*X*Z output of the final Ux Uz Px Pz Sx Sz. */
+int ouc_forward(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gather_vx, float* gather_vz,
+                float* fields);
+int ouc_forward_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, float* d_gather_vx,
+                    float* d_gather_vz);
+
+/* One RTM shot: forward with boundary-strip save (PS:2258-2292), optional
+ * mute (PS:2293), receiver back-propagation with record injection and the
+ * source-wavefield reconstruction (PS:2313-2364), PP/PS imaging (PS:2361),
+ * normalisation and Laplacian (PS:2367-2373).  rec_vx/rec_vz are the
+ * observed records (X*nt, cfg->gather_layout); NULL uses the records the
+ * forward pass produces, as the reference's main() does.  img_pp/img_ps
+ * receive the nx*nz Laplacian-filtered images (the per-shot files of
+ * PS:2379-2400); either may be NULL.  The images are also added into the
+ * context's FP64 stack. */
+int ouc_rtm_shot(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rec_vx,
+                 const float* rec_vz, float* img_pp, float* img_ps);
+int ouc_rtm_shot_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, const float* d_rec_vx,
+                     const float* d_rec_vz, float* d_img_pp, float* d_img_ps);
+
+/* FP64 cross-shot stack of the Laplacian images (replaces the host FP32 sum
+ * through per-shot files, PS:2403-2443) and the FP64 stacked illumination.
+ * Any output may be NULL; reset != 0 clears the stack after reading. */
+int ouc_stack(ouc_ctx* ctx, double* stack_pp, double* stack_ps, double* illum, int reset);
+int ouc_stack_dev(ouc_ctx* ctx, const double** d_pp, const double** d_ps, const double** d_illum);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OUC_H */

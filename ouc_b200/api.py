@@ -1,0 +1,202 @@
+"""Python mirror of the modeling / RTM operator surface (include/ouc.h).
+
+The reference exposes no library API; its operator surface is the set of
+kernels its main() drives (P-S-seperating.cu:2258-2376).  ``Context`` owns
+one model on the device and offers the two operations that main() performs
+per shot -- forward modeling with receiver extraction, and one RTM shot --
+plus the cross-shot stack.  Arrays are numpy, x-major with z contiguous.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+MODEL_INTERIOR, MODEL_PADDED = 0, 1
+STRIP_REFERENCE, STRIP_EXACT = 0, 1
+IMAGE_REFERENCE, IMAGE_EXACT = 0, 1
+PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
+SRC_THETA, SRC_FORCE_Z = 0, 1
+GATHER_XT, GATHER_TX = 0, 1
+
+
+@dataclass
+class Config:
+    nx: int
+    nz: int
+    npml: int
+    dx: float
+    dz: float
+    dt: float
+    nt: int
+    half_order: int = 5
+    pml_r: float = 1e-3
+    model_layout: int = MODEL_INTERIOR
+    strip_level: int = STRIP_REFERENCE
+    image_align: int = IMAGE_REFERENCE
+    strip_precision: int = PREC_FP32
+    compensated_image: int = 0
+    gather_layout: int = GATHER_XT
+    device: int = 0
+    stream: int = 0
+
+    def c(self):
+        c = _lib.ouc_config()
+        for name, _ in _lib.ouc_config._fields_:
+            v = getattr(self, name)
+            setattr(c, name, v if name != "stream" else (v or None))
+        return c
+
+    @property
+    def X(self):
+        return self.nx + 2 * self.npml
+
+    @property
+    def Z(self):
+        return self.nz + 2 * self.npml
+
+
+@dataclass
+class Shot:
+    sx: int
+    sz: int
+    rz: int
+    src_type: int = SRC_THETA
+    t0: int = 0
+    mute: int = 1
+
+    def c(self):
+        return _lib.ouc_shot(self.sx, self.sz, self.rz, self.src_type, self.t0, self.mute)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def stencil_weights(n):
+    out = np.zeros(n, np.float32)
+    check(lib().ouc_stencil_weights(n, _p(out)))
+    return out
+
+
+def ricker(fm, dt, nt):
+    """Ricker wavelet as the reference builds it (P-S-seperating.cu:1954-1958)."""
+    out = np.zeros(nt, np.float32)
+    t0 = C.c_int()
+    check(lib().ouc_ricker(fm, dt, nt, _p(out), C.byref(t0)))
+    return out, t0.value
+
+
+class Context:
+    """One model resident on one B200; shots run on the context's stream."""
+
+    def __init__(self, cfg: Config, vp, vs, rho=None):
+        self.cfg = cfg
+        vp, vs = _f32(vp), _f32(vs)
+        rho = None if rho is None else _f32(rho)
+        want = (cfg.X, cfg.Z) if cfg.model_layout == MODEL_PADDED else (cfg.nx, cfg.nz)
+        if vp.shape != want or vs.shape != want:
+            raise ValueError(f"model shape {vp.shape} / {vs.shape}, expected {want}")
+        h = C.c_void_p()
+        cc = cfg.c()
+        rc = lib().ouc_create(C.byref(cc), _p(vp), _p(vs), _p(rho), C.byref(h))
+        if rc != 0:
+            raise _lib.OucError(rc, "ouc_create")
+        self._h = h
+        X, Z = C.c_int(), C.c_int()
+        check(lib().ouc_dims(h, C.byref(X), C.byref(Z)), h)
+        self.X, self.Z = X.value, Z.value
+
+    # ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ouc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self):
+        return lib().ouc_stream(self._h)
+
+    def device_bytes(self):
+        return int(lib().ouc_device_bytes(self._h))
+
+    def timing(self):
+        t = _lib.ouc_timing()
+        check(lib().ouc_last_timing(self._h, C.byref(t)), self._h)
+        return dict(forward_ms=t.forward_ms, backward_ms=t.backward_ms, finalize_ms=t.finalize_ms,
+                    copy_ms=t.copy_ms, kernel_launches=int(t.kernel_launches))
+
+    def _gshape(self):
+        nt = self.cfg.nt
+        return (self.X, nt) if self.cfg.gather_layout == GATHER_XT else (nt, self.X)
+
+    # ------------------------------------------------------------------
+    def forward(self, shot: Shot, wavelet, fields=False):
+        """Forward modeling: (gather_vx, gather_vz, fields or None).
+
+        fields: final Ux, Uz, Px, Pz, Sx, Sz on the padded grid, (6, X, Z)."""
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        gx = np.zeros(self._gshape(), np.float32)
+        gz = np.zeros(self._gshape(), np.float32)
+        f = np.zeros((6, self.X, self.Z), np.float32) if fields else None
+        sc = shot.c()
+        check(lib().ouc_forward(self._h, C.byref(sc), _p(w), _p(gx), _p(gz), _p(f)), self._h)
+        return gx, gz, f
+
+    def rtm_shot(self, shot: Shot, wavelet, rec=None):
+        """One RTM shot; rec = (rec_vx, rec_vz) in the configured gather layout,
+        or None to migrate the records this shot's own forward pass produces."""
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        rx = rz = None
+        if rec is not None:
+            rx, rz = _f32(rec[0]), _f32(rec[1])
+            assert rx.shape == self._gshape() and rz.shape == self._gshape()
+        pp = np.zeros((self.cfg.nx, self.cfg.nz), np.float32)
+        ps = np.zeros((self.cfg.nx, self.cfg.nz), np.float32)
+        sc = shot.c()
+        check(lib().ouc_rtm_shot(self._h, C.byref(sc), _p(w), _p(rx), _p(rz), _p(pp), _p(ps)), self._h)
+        return pp, ps
+
+    def rtm_shot_dev(self, shot: Shot, d_wavelet, d_rec_vx=None, d_rec_vz=None, d_img_pp=None, d_img_ps=None):
+        """Device-pointer variant (integers); no host copies."""
+        sc = shot.c()
+        check(lib().ouc_rtm_shot_dev(self._h, C.byref(sc), d_wavelet, d_rec_vx, d_rec_vz, d_img_pp, d_img_ps),
+              self._h)
+
+    def forward_dev(self, shot: Shot, d_wavelet, d_gx=None, d_gz=None):
+        sc = shot.c()
+        check(lib().ouc_forward_dev(self._h, C.byref(sc), d_wavelet, d_gx, d_gz), self._h)
+
+    def stack(self, reset=False):
+        n = (self.cfg.nx, self.cfg.nz)
+        pp, ps, il = np.zeros(n), np.zeros(n), np.zeros(n)
+        dp = C.POINTER(C.c_double)
+        check(lib().ouc_stack(self._h, pp.ctypes.data_as(dp), ps.ctypes.data_as(dp), il.ctypes.data_as(dp),
+                              int(reset)), self._h)
+        return pp, ps, il

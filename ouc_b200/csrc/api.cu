@@ -1,0 +1,687 @@
+// C ABI of libouc.so: context, device memory and the per-shot time loops.
+//
+// Host-side orchestration that replaces the reference's main() (PS:1658-2401)
+// for the modeling and RTM path: model padding and damping profile, the
+// forward loop with boundary-strip save, the mute, the backward loop that
+// back-propagates the records and reconstructs the source wavefield, the
+// imaging condition and the per-shot image finalisation with an FP64 stack.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ouc.h"
+#include "ouc_internal.h"
+
+using namespace ouc;
+
+namespace {
+
+// Float32 staggered weights.  N = 6: the reference's literals (PS:221).
+// Other N: the exact Taylor solution of sum_k c_k (2k-1)^(2n-1) = [n==1],
+// rounded to float32.
+const double kWeights[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {1.0, 0, 0, 0, 0, 0},
+    {1.125, -1.0 / 24.0, 0, 0, 0, 0},
+    {75.0 / 64.0, -25.0 / 384.0, 3.0 / 640.0, 0, 0, 0},
+    {1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0, 0, 0},
+    {19845.0 / 16384.0, -735.0 / 8192.0, 567.0 / 40960.0, -405.0 / 229376.0, 35.0 / 294912.0, 0},
+    {1.2213364, -9.6931458e-2, 1.7447662e-2, -2.9672895e-3, 3.5900540e-4, -2.1847812e-5},
+};
+
+struct Side {
+    float* now[4];
+    float* past[4];
+    float* fo[4];
+    float* fn[4];
+    float* o[8];
+    float* base;      // first field of the side (for zeroing)
+    size_t floats;    // span of the side's fields
+    void swap_levels() { for (int k = 0; k < 4; ++k) std::swap(now[k], past[k]); }
+    void swap_memory() { for (int k = 0; k < 4; ++k) std::swap(fo[k], fn[k]); }
+};
+
+}  // namespace
+
+struct ouc_ctx {
+    ouc_config cfg;
+    int X = 0, Z = 0, L = 0, N = 0, nx = 0, nz = 0, nt = 0;
+    int Xc = 0, Zc = 0, pitch = 0;
+    size_t fstride = 0;          // floats per field allocation
+    int tiles_x = 0, tiles_z = 0;
+    int rec_tx0 = 0, rec_tz0 = 0, rec_tiles_x = 0, rec_tiles_z = 0;
+    float a[6] = {0, 0, 0, 0, 0, 0};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    std::string err;
+    ouc_timing timing{};
+    Ring ring{};
+    std::vector<float> vp_host;  // padded Vp (for the mute's velocity)
+
+    // device memory
+    float* arena = nullptr;
+    size_t arena_floats = 0;
+    float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
+    Side src{}, rcv{};
+    float* acc[3] = {nullptr, nullptr, nullptr};
+    float* gather[2] = {nullptr, nullptr};    // time-major [nt][X]
+    float* staging = nullptr;                  // 2*nt*X floats for transposes / packing
+    float* d_wavelet = nullptr;
+    float* d_img[2] = {nullptr, nullptr};
+    double* d_stack[3] = {nullptr, nullptr, nullptr};
+    float* strips = nullptr;
+    size_t strip_slot = 0;                     // floats per slot
+    size_t bytes = 0;
+    bool stacked = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    float* field(size_t k) const { return arena + k * fstride + (size_t)kGX * pitch + kZOFF; }
+};
+
+namespace {
+
+int fail(ouc_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(ouc_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, OUC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);   \
+    } while (0)
+
+// Edge padding of the interior model into the absorbing layer, as the
+// reference's xiangbian (PS:37-119): sides copy the nearest interior
+// row/column, corners the nearest interior corner cell.
+void pad_edges(std::vector<float>& f, int X, int Z, int L) {
+    auto at = [&](int i, int j) -> float& { return f[(size_t)i * Z + j]; };
+    for (int i = L; i < X - L; ++i) {
+        for (int j = 0; j < L; ++j) at(i, j) = at(i, L);
+        for (int j = Z - L; j < Z; ++j) at(i, j) = at(i, Z - L - 1);
+    }
+    for (int j = L; j < Z - L; ++j) {
+        for (int i = 0; i < L; ++i) at(i, j) = at(L, j);
+        for (int i = X - L; i < X; ++i) at(i, j) = at(X - L - 1, j);
+    }
+    for (int i = 0; i < X; ++i) {
+        if (i >= L && i < X - L) continue;
+        for (int j = 0; j < Z; ++j) {
+            if (j >= L && j < Z - L) continue;
+            at(i, j) = at(i < L ? L : X - L - 1, j < L ? L : Z - L - 1);
+        }
+    }
+}
+
+// Damping profile of PS:2067-2105: d = log10(1/R) * 1.5 * Vp / L *
+// (dist/L)^4 with L in cells, computed in double and stored as float.
+// Left/top layers hold L damped cells, right/bottom L-1 (strict ">").
+void damping(const std::vector<float>& vp, int X, int Z, int L, double R, std::vector<float>& ax,
+             std::vector<float>& az) {
+    const double g = log10(1.0 / R) * 1.5;
+    for (int i = 0; i < X; ++i)
+        for (int j = 0; j < Z; ++j) {
+            const size_t c = (size_t)i * Z + j;
+            const double v = vp[c];
+            if (i < L) ax[c] = (float)(g * v / L * pow(1.0 * (L - i) / L, 4.0));
+            else if (i > X - L) ax[c] = (float)(g * v / L * pow(1.0 * (i - X + L) / L, 4.0));
+            else ax[c] = 0.f;
+            if (j < L) az[c] = (float)(g * v / L * pow(1.0 * (L - j) / L, 4.0));
+            else if (j > Z - L) az[c] = (float)(g * v / L * pow(1.0 * (j - Z + L) / L, 4.0));
+            else az[c] = 0.f;
+        }
+}
+
+int upload_field(ouc_ctx* ctx, float* dst, const float* host) {
+    CK(cudaMemcpy2DAsync(dst, (size_t)ctx->pitch * 4, host, (size_t)ctx->Z * 4, (size_t)ctx->Z * 4, ctx->X,
+                         cudaMemcpyHostToDevice, ctx->stream));
+    return OUC_OK;
+}
+
+StepArgs base_args(const ouc_ctx* c) {
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.X = c->X; a.Z = c->Z; a.pitch = c->pitch; a.L = c->L;
+    a.tiles_z = c->tiles_z; a.tile_x0 = 0; a.tile_z0 = 0;
+    for (int k = 0; k < 6; ++k) a.a[k] = c->a[k];
+    a.dx = c->cfg.dx; a.dz = c->cfg.dz; a.dt = c->cfg.dt;
+    a.dt2 = c->cfg.dt * c->cfg.dt;
+    a.vp2 = c->vp2; a.vs2 = c->vs2; a.ax = c->ax; a.az = c->az;
+    a.ring = c->ring;
+    return a;
+}
+
+void bind_side(StepArgs& a, const Side& s) {
+    for (int k = 0; k < 4; ++k) {
+        a.now[k] = s.now[k]; a.past[k] = s.past[k];
+        a.f_old[k] = s.fo[k]; a.f_new[k] = s.fn[k];
+    }
+    for (int k = 0; k < 8; ++k) a.o[k] = s.o[k];
+}
+
+int check_shot(ouc_ctx* ctx, const ouc_shot* s) {
+    if (!s) return fail(ctx, OUC_EINVAL, "shot is NULL");
+    if (s->sx < 0 || s->sx >= ctx->nx || s->sz < 0 || s->sz >= ctx->nz)
+        return fail(ctx, OUC_EINVAL, "source outside the interior grid");
+    if (s->rz < 0 || s->rz >= ctx->nz) return fail(ctx, OUC_EINVAL, "receiver row outside the interior grid");
+    if (s->src_type != OUC_SRC_THETA && s->src_type != OUC_SRC_FORCE_Z)
+        return fail(ctx, OUC_EINVAL, "unknown source type");
+    return OUC_OK;
+}
+
+int ensure_strips(ouc_ctx* ctx) {
+    if (ctx->strips) return OUC_OK;
+    ctx->strip_slot = (size_t)kStripFields * ctx->ring.R;
+    size_t bytes = ctx->strip_slot * (size_t)ctx->nt * sizeof(float);
+    cudaError_t e = cudaMalloc(&ctx->strips, bytes);
+    if (e != cudaSuccess) {
+        ctx->strips = nullptr;
+        cudaGetLastError();
+        return fail(ctx, OUC_ENOMEM, "cannot allocate boundary strips (" + std::to_string(bytes >> 20) + " MiB)");
+    }
+    ctx->bytes += bytes;
+    return OUC_OK;
+}
+
+// Forward time loop (PS:2258-2292).  Records into the time-major gathers when
+// `record`, saves the boundary ring of every step when `save`.
+int run_forward(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, bool record, bool save) {
+    Side& s = ctx->src;
+    CK(cudaMemsetAsync(s.base, 0, s.floats * sizeof(float), ctx->stream));
+    StepArgs a = base_args(ctx);
+    a.sx = shot->sx + ctx->L; a.sz = shot->sz + ctx->L;
+    a.src_type = shot->src_type;
+    a.wavelet = d_wavelet;
+    a.rz = shot->rz + ctx->L;
+    for (int t = 0; t < ctx->nt; ++t) {
+        bind_side(a, s);
+        a.t = t; a.src_t = t;
+        a.rec_x = record ? ctx->gather[0] + (size_t)t * ctx->X : nullptr;
+        a.rec_z = record ? ctx->gather[1] + (size_t)t * ctx->X : nullptr;
+        a.strip_save = save ? ctx->strips + (size_t)t * ctx->strip_slot : nullptr;
+        if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+        s.swap_levels();
+        s.swap_memory();
+    }
+    ctx->timing.kernel_launches += ctx->nt;
+    CK(cudaGetLastError());
+    return OUC_OK;
+}
+
+// Backward loop (PS:2313-2364) and imaging; the source-side state holds the
+// forward's last two levels on entry.
+int run_backward(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet) {
+    Side& s = ctx->src;
+    Side& r = ctx->rcv;
+    const int nt = ctx->nt;
+    CK(cudaMemsetAsync(r.base, 0, r.floats * sizeof(float), ctx->stream));
+    for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->acc[k] - (size_t)kGX * ctx->pitch - kZOFF, 0,
+                                                   ctx->fstride * sizeof(float), ctx->stream));
+    StepArgs ar = base_args(ctx);
+    ar.rz = shot->rz + ctx->L;
+    StepArgs as = base_args(ctx);
+    as.tiles_z = ctx->rec_tiles_z; as.tile_x0 = ctx->rec_tx0; as.tile_z0 = ctx->rec_tz0;
+    as.sx = shot->sx + ctx->L; as.sz = shot->sz + ctx->L;
+    as.wavelet = d_wavelet;
+    as.img_past = ctx->cfg.image_align == OUC_IMAGE_REFERENCE;
+    for (int k = 0; k < 3; ++k) as.acc[k] = ctx->acc[k];
+    const bool exact = ctx->cfg.strip_level == OUC_STRIP_EXACT;
+    // theta-type source only: a force source does not enter the S-stage
+    const bool theta_src = shot->src_type == OUC_SRC_THETA;
+    long long launches = 0;
+    for (int t = nt - 1; t >= 0; --t) {
+        // receiver side: injection + S/U stages with damping (PS:2319-2324, 2349-2354)
+        bind_side(ar, r);
+        ar.t = t;
+        ar.inj_x = ctx->gather[0] + (size_t)t * ctx->X;
+        ar.inj_z = ctx->gather[1] + (size_t)t * ctx->X;
+        if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+        r.swap_levels();
+        r.swap_memory();
+        ++launches;
+        if (t == nt - 1) {
+            // no reconstruction at the last level: correlate the forward's final P
+            StepArgs ai = base_args(ctx);
+            for (int k = 0; k < 4; ++k) { ai.now[k] = s.now[k]; ai.rcv[k] = r.now[k]; }
+            for (int k = 0; k < 3; ++k) ai.acc[k] = ctx->acc[k];
+            launch_image_only(ai, ctx->stream);
+            ++launches;
+            s.swap_levels();   // now = level NT-1, past = level NT
+            continue;
+        }
+        // source side: inverse leapfrog on the interior from level t+1 and t+2
+        bind_side(as, s);
+        as.t = t;
+        as.src_t = t + 1;
+        as.src_recon = theta_src && (exact || t + 1 == nt - 1);
+        const int slot_u = exact ? t : (t + 1 == nt - 1 ? nt - 2 : t + 1);
+        as.strip_u = ctx->strips + (size_t)slot_u * ctx->strip_slot;
+        as.strip_s = ctx->strips + (size_t)(t + 1) * ctx->strip_slot;
+        for (int k = 0; k < 4; ++k) as.rcv[k] = r.now[k];
+        if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+        s.swap_levels();
+        ++launches;
+    }
+    ctx->timing.kernel_launches += launches;
+    CK(cudaGetLastError());
+    return OUC_OK;
+}
+
+int finalize(ouc_ctx* ctx, float* d_pp, float* d_ps) {
+    FinalizeArgs f;
+    f.X = ctx->X; f.Z = ctx->Z; f.pitch = ctx->pitch; f.L = ctx->L;
+    f.dh = ctx->cfg.dx;   // main() passes dx as the Laplacian spacing (PS:2372)
+    for (int k = 0; k < 3; ++k) { f.acc[k] = ctx->acc[k]; f.stack[k] = ctx->d_stack[k]; }
+    f.img_pp = d_pp; f.img_ps = d_ps;
+    launch_finalize(f, ctx->stream);
+    ctx->timing.kernel_launches += 1;
+    ctx->stacked = true;
+    CK(cudaGetLastError());
+    return OUC_OK;
+}
+
+// Bring a gather from the caller's layout into the time-major device gather.
+int gather_in(ouc_ctx* ctx, const float* src, float* dst_tx, bool host) {
+    const size_t n = (size_t)ctx->nt * ctx->X;
+    const bool xt = ctx->cfg.gather_layout == OUC_GATHER_XT;
+    if (!xt) {
+        CK(cudaMemcpyAsync(dst_tx, src, n * 4, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+        return OUC_OK;
+    }
+    const float* from = src;
+    if (host) {
+        CK(cudaMemcpyAsync(ctx->staging, src, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+        from = ctx->staging;
+    }
+    launch_transpose(from, dst_tx, ctx->X, ctx->nt, ctx->stream);   // [X][nt] -> [nt][X]
+    ctx->timing.kernel_launches += 1;
+    return OUC_OK;
+}
+
+int gather_out(ouc_ctx* ctx, const float* src_tx, float* dst, bool host) {
+    const size_t n = (size_t)ctx->nt * ctx->X;
+    const bool xt = ctx->cfg.gather_layout == OUC_GATHER_XT;
+    const float* from = src_tx;
+    if (xt) {
+        float* tgt = host ? ctx->staging : dst;
+        launch_transpose(src_tx, tgt, ctx->nt, ctx->X, ctx->stream);   // [nt][X] -> [X][nt]
+        ctx->timing.kernel_launches += 1;
+        from = tgt;
+        if (!host) return OUC_OK;
+    }
+    CK(cudaMemcpyAsync(dst, from, n * 4, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+    return OUC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ouc_strerror(int status) {
+    switch (status) {
+        case OUC_OK: return "ok";
+        case OUC_EINVAL: return "invalid argument";
+        case OUC_ECUDA: return "CUDA runtime error";
+        case OUC_ENOMEM: return "device out of memory";
+        case OUC_EUNSTABLE: return "unstable configuration (CFL) or non-finite wavefield";
+        case OUC_ESTATE: return "call out of order";
+        case OUC_ETIMEOUT: return "device wait timed out";
+        case OUC_ENODEV: return "no usable sm_100 device";
+    }
+    return "unknown status";
+}
+
+const char* ouc_last_error(const ouc_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int ouc_version(void) { return OUC_VERSION_MAJOR * 100 + OUC_VERSION_MINOR; }
+
+int ouc_stencil_weights(int half_order, float* out) {
+    if (half_order < 1 || half_order > 6 || !out) return OUC_EINVAL;
+    for (int k = 0; k < half_order; ++k) out[k] = (float)kWeights[half_order][k];
+    return OUC_OK;
+}
+
+int ouc_ricker(float fm, float dt, int nt, float* out, int* t0_out) {
+    if (!(fm > 0) || !(dt > 0) || nt < 1 || !out) return OUC_EINVAL;
+    const double pi_ref = 3.1415926;   // PS:14
+    const double f = fm;
+    const float nk = (float)(pi_ref * pi_ref * f * f * dt * dt);
+    const int t0 = (int)ceil(1.0 / (f * dt));
+    for (int t = 0; t < nt; ++t) {
+        const int d = t - t0;
+        const float e = std::exp(-nk * d * d);   // float exponent, as in PS:1958
+        out[t] = (float)((1.0 - 2.0 * nk * d * d) * e);
+    }
+    if (t0_out) *t0_out = t0;
+    return OUC_OK;
+}
+
+int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const float* rho, ouc_ctx** out) {
+    (void)rho;   // density does not enter the reference's equations (PS:373-378)
+    if (!cfg || !vp || !vs || !out) return OUC_EINVAL;
+    *out = nullptr;
+    ouc_ctx* ctx = new (std::nothrow) ouc_ctx();
+    if (!ctx) return OUC_ENOMEM;
+    ctx->cfg = *cfg;
+    const int N = cfg->half_order, L = cfg->npml;
+    auto bad = [&](const char* m) { ctx->err = m; int rc = OUC_EINVAL; ouc_destroy(ctx); return rc; };
+    if (N != 2 && N != 4 && N != 5 && N != 6) return bad("half_order must be 2, 4, 5 or 6");
+    if (cfg->nx < 4 * N || cfg->nz < 4 * N) return bad("interior must be at least 4N cells in each direction");
+    if (L < N) return bad("npml must be at least the stencil half-width");
+    if (!(cfg->dx > 0) || !(cfg->dz > 0) || !(cfg->dt > 0) || cfg->nt < 2) return bad("bad spacing, time step or nt");
+    if (!(cfg->pml_r > 0 && cfg->pml_r < 1)) return bad("pml_r must be in (0, 1)");
+    ctx->N = N; ctx->L = L; ctx->nx = cfg->nx; ctx->nz = cfg->nz; ctx->nt = cfg->nt;
+    ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
+    for (int k = 0; k < N; ++k) ctx->a[k] = (float)kWeights[N][k];
+    const int X = ctx->X, Z = ctx->Z;
+
+    // model on the padded grid
+    std::vector<float> P_vp((size_t)X * Z), P_vs((size_t)X * Z);
+    if (cfg->model_layout == OUC_MODEL_PADDED) {
+        std::copy(vp, vp + (size_t)X * Z, P_vp.begin());
+        std::copy(vs, vs + (size_t)X * Z, P_vs.begin());
+    } else {
+        for (int i = 0; i < cfg->nx; ++i)
+            for (int j = 0; j < cfg->nz; ++j) {
+                P_vp[(size_t)(i + L) * Z + j + L] = vp[(size_t)i * cfg->nz + j];
+                P_vs[(size_t)(i + L) * Z + j + L] = vs[(size_t)i * cfg->nz + j];
+            }
+        pad_edges(P_vp, X, Z, L);
+        pad_edges(P_vs, X, Z, L);
+    }
+    float vmax = 0.f;
+    for (float v : P_vp) {
+        if (!(v > 0) || !std::isfinite(v)) return bad("Vp must be positive and finite");
+        vmax = std::max(vmax, v);
+    }
+    for (float v : P_vs)
+        if (!(v >= 0) || !std::isfinite(v)) return bad("Vs must be non-negative and finite");
+    // stability of the staggered leapfrog: dt vmax sum|a_k| sqrt(1/dx^2 + 1/dz^2) <= 1
+    double sa = 0;
+    for (int k = 0; k < N; ++k) sa += fabs(kWeights[N][k]);
+    const double cfl = cfg->dt * vmax * sa * sqrt(1.0 / (cfg->dx * cfg->dx) + 1.0 / (cfg->dz * cfg->dz));
+    if (cfl > 1.0) {
+        ctx->err = "CFL number " + std::to_string(cfl) + " > 1 for this dt";
+        ouc_destroy(ctx);
+        return OUC_EUNSTABLE;
+    }
+    std::vector<float> hax((size_t)X * Z), haz((size_t)X * Z);
+    damping(P_vp, X, Z, L, cfg->pml_r, hax, haz);
+    ctx->vp_host = P_vp;
+    std::vector<float> vp2((size_t)X * Z), vs2((size_t)X * Z);
+    for (size_t k = 0; k < vp2.size(); ++k) { vp2[k] = P_vp[k] * P_vp[k]; vs2[k] = P_vs[k] * P_vs[k]; }
+
+    // device
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0) {
+        cudaGetLastError();
+        ctx->err = "no CUDA device";
+        ouc_destroy(ctx);
+        return OUC_ENODEV;
+    }
+    ctx->device = cfg->device;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) { ctx->err = "cudaSetDevice failed"; ouc_destroy(ctx); return OUC_ENODEV; }
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, ctx->device);
+    if (prop.major != 10) {
+        ctx->err = std::string("device ") + prop.name + " is not sm_100";
+        ouc_destroy(ctx);
+        return OUC_ENODEV;
+    }
+    if (cfg->stream) {
+        ctx->stream = (cudaStream_t)cfg->stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            ctx->err = "cannot create stream"; ouc_destroy(ctx); return OUC_ECUDA;
+        }
+        ctx->own_stream = true;
+    }
+    for (auto& e : ctx->ev) cudaEventCreate(&e);
+
+    // layout
+    const int TX = 32, TZ = 64;
+    ctx->tiles_x = (X + TX - 1) / TX; ctx->tiles_z = (Z + TZ - 1) / TZ;
+    ctx->Xc = ctx->tiles_x * TX; ctx->Zc = ctx->tiles_z * TZ;
+    ctx->pitch = ((kZOFF + ctx->Zc + kZOFF) + 31) / 32 * 32;
+    ctx->fstride = (size_t)(ctx->Xc + 2 * kGX) * ctx->pitch;
+    ctx->rec_tx0 = L / TX; ctx->rec_tz0 = L / TZ;
+    ctx->rec_tiles_x = (X - L - 1) / TX - ctx->rec_tx0 + 1;
+    ctx->rec_tiles_z = (Z - L - 1) / TZ - ctx->rec_tz0 + 1;
+    ctx->ring = Ring::make(X, Z, L, N);
+
+    // fields: model 4, source side 24, receiver side 24, accumulators 3
+    const int nfields = 4 + 24 + 24 + 3;
+    ctx->arena_floats = ctx->fstride * nfields;
+    size_t arena_bytes = ctx->arena_floats * sizeof(float);
+    if (cudaMalloc(&ctx->arena, arena_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "cannot allocate wavefield state";
+        ouc_destroy(ctx);
+        return OUC_ENOMEM;
+    }
+    ctx->bytes += arena_bytes;
+    cudaMemsetAsync(ctx->arena, 0, arena_bytes, ctx->stream);
+    size_t k = 0;
+    ctx->vp2 = ctx->field(k++); ctx->vs2 = ctx->field(k++); ctx->ax = ctx->field(k++); ctx->az = ctx->field(k++);
+    for (Side* s : {&ctx->src, &ctx->rcv}) {
+        s->base = ctx->arena + k * ctx->fstride;
+        s->floats = 24 * ctx->fstride;
+        for (int q = 0; q < 4; ++q) s->now[q] = ctx->field(k++);
+        for (int q = 0; q < 4; ++q) s->past[q] = ctx->field(k++);
+        for (int q = 0; q < 4; ++q) s->fo[q] = ctx->field(k++);
+        for (int q = 0; q < 4; ++q) s->fn[q] = ctx->field(k++);
+        for (int q = 0; q < 8; ++q) s->o[q] = ctx->field(k++);
+    }
+    for (int q = 0; q < 3; ++q) ctx->acc[q] = ctx->field(k++);
+
+    const size_t ng = (size_t)ctx->nt * X;
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    bool ok = cudaMalloc(&ctx->gather[0], ng * 4) == cudaSuccess && cudaMalloc(&ctx->gather[1], ng * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->staging, std::max(ng, (size_t)6 * X * Z) * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->d_wavelet, (size_t)ctx->nt * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->d_img[0], ni * 4) == cudaSuccess && cudaMalloc(&ctx->d_img[1], ni * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->d_stack[0], ni * 8) == cudaSuccess && cudaMalloc(&ctx->d_stack[1], ni * 8) == cudaSuccess &&
+              cudaMalloc(&ctx->d_stack[2], ni * 8) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        ctx->err = "cannot allocate gathers, images or stack";
+        ouc_destroy(ctx);
+        return OUC_ENOMEM;
+    }
+    ctx->bytes += 2 * ng * 4 + std::max(ng, (size_t)6 * X * Z) * 4 + (size_t)ctx->nt * 4 + 2 * ni * 4 + 3 * ni * 8;
+    for (int q = 0; q < 3; ++q) cudaMemsetAsync(ctx->d_stack[q], 0, ni * 8, ctx->stream);
+    int rc = OUC_OK;
+    if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
+        (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data()))) {
+        ouc_destroy(ctx);
+        return rc;
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        ctx->err = "setup failed";
+        ouc_destroy(ctx);
+        return OUC_ECUDA;
+    }
+    *out = ctx;
+    return OUC_OK;
+}
+
+int ouc_destroy(ouc_ctx* ctx) {
+    if (!ctx) return OUC_OK;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->arena);
+    cudaFree(ctx->gather[0]); cudaFree(ctx->gather[1]);
+    cudaFree(ctx->staging); cudaFree(ctx->d_wavelet);
+    cudaFree(ctx->d_img[0]); cudaFree(ctx->d_img[1]);
+    for (auto* p : ctx->d_stack) cudaFree(p);
+    cudaFree(ctx->strips);
+    for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return OUC_OK;
+}
+
+int ouc_dims(const ouc_ctx* ctx, int* X, int* Z) {
+    if (!ctx) return OUC_EINVAL;
+    if (X) *X = ctx->X;
+    if (Z) *Z = ctx->Z;
+    return OUC_OK;
+}
+
+void* ouc_stream(const ouc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int ouc_last_timing(const ouc_ctx* ctx, ouc_timing* t) {
+    if (!ctx || !t) return OUC_EINVAL;
+    *t = ctx->timing;
+    return OUC_OK;
+}
+
+size_t ouc_device_bytes(const ouc_ctx* ctx) { return ctx ? ctx->bytes : 0; }
+
+static int forward_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gx, float* gz,
+                        float* fields, bool host) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = check_shot(ctx, shot);
+    if (rc) return rc;
+    if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
+    cudaSetDevice(ctx->device);
+    ctx->timing = ouc_timing{};
+    const float* d_w = wavelet;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    if (host) {
+        CK(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
+        d_w = ctx->d_wavelet;
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    if ((rc = run_forward(ctx, shot, d_w, gx || gz, false))) return rc;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    if (gx && (rc = gather_out(ctx, ctx->gather[0], gx, host))) return rc;
+    if (gz && (rc = gather_out(ctx, ctx->gather[1], gz, host))) return rc;
+    if (fields && host) {
+        const float* f[4] = {ctx->src.now[0], ctx->src.now[1], ctx->src.now[2], ctx->src.now[3]};
+        launch_pack_fields(f, 4, ctx->X, ctx->Z, ctx->pitch, ctx->staging, ctx->stream);
+        const size_t C = (size_t)ctx->X * ctx->Z;
+        CK(cudaMemcpyAsync(fields + 2 * C, ctx->staging, 4 * C * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (fields && host) {
+        const size_t C = (size_t)ctx->X * ctx->Z;
+        for (size_t k = 0; k < C; ++k) {
+            fields[k] = fields[2 * C + k] + fields[4 * C + k];       // Ux = Px + Sx
+            fields[C + k] = fields[3 * C + k] + fields[5 * C + k];   // Uz = Pz + Sz
+        }
+    }
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
+    ctx->timing.forward_ms = b;
+    ctx->timing.copy_ms = a + c;
+    return OUC_OK;
+}
+
+int ouc_forward(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gx, float* gz, float* fields) {
+    return forward_impl(ctx, shot, wavelet, gx, gz, fields, true);
+}
+
+int ouc_forward_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, float* d_gx, float* d_gz) {
+    return forward_impl(ctx, shot, d_wavelet, d_gx, d_gz, nullptr, false);
+}
+
+static int rtm_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rx, const float* rz,
+                    float* img_pp, float* img_ps, bool host) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = check_shot(ctx, shot);
+    if (rc) return rc;
+    if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
+    if ((rx == nullptr) != (rz == nullptr)) return fail(ctx, OUC_EINVAL, "give both record components or neither");
+    cudaSetDevice(ctx->device);
+    if ((rc = ensure_strips(ctx))) return rc;
+    ctx->timing = ouc_timing{};
+    const float* d_w = wavelet;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    if (host) {
+        CK(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
+        d_w = ctx->d_wavelet;
+    }
+    if ((rc = run_forward(ctx, shot, d_w, rx == nullptr, true))) return rc;
+    if (rx) {
+        if ((rc = gather_in(ctx, rx, ctx->gather[0], host))) return rc;
+        if ((rc = gather_in(ctx, rz, ctx->gather[1], host))) return rc;
+    }
+    if (shot->mute) {
+        const int sx = shot->sx + ctx->L, sz = shot->sz + ctx->L, rzz = shot->rz + ctx->L;
+        const float v = ctx->vp_host[(size_t)sx * ctx->Z + rzz];   // Vp at (Sx, Z_receive), PS:1645
+        launch_mute(ctx->gather[0], ctx->gather[1], ctx->X, ctx->nt, sx, sz, rzz, shot->t0, ctx->cfg.dt, ctx->cfg.dx, v,
+                    ctx->stream);
+        ctx->timing.kernel_launches += 1;
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    if ((rc = run_backward(ctx, shot, d_w))) return rc;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    float* d_pp = host ? ctx->d_img[0] : img_pp;
+    float* d_ps = host ? ctx->d_img[1] : img_ps;
+    if ((rc = finalize(ctx, d_pp, d_ps))) return rc;
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    if (host && img_pp) CK(cudaMemcpyAsync(img_pp, d_pp, ni * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (host && img_ps) CK(cudaMemcpyAsync(img_ps, d_ps, ni * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
+    ctx->timing.forward_ms = a;
+    ctx->timing.backward_ms = b;
+    ctx->timing.finalize_ms = c;
+    return OUC_OK;
+}
+
+int ouc_rtm_shot(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rx, const float* rz,
+                 float* img_pp, float* img_ps) {
+    return rtm_impl(ctx, shot, wavelet, rx, rz, img_pp, img_ps, true);
+}
+
+int ouc_rtm_shot_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, const float* d_rx, const float* d_rz,
+                     float* d_img_pp, float* d_img_ps) {
+    if (ctx && (!d_img_pp || !d_img_ps)) {
+        d_img_pp = d_img_pp ? d_img_pp : ctx->d_img[0];
+        d_img_ps = d_img_ps ? d_img_ps : ctx->d_img[1];
+    }
+    return rtm_impl(ctx, shot, d_wavelet, d_rx, d_rz, d_img_pp, d_img_ps, false);
+}
+
+int ouc_stack(ouc_ctx* ctx, double* pp, double* ps, double* illum, int reset) {
+    if (!ctx) return OUC_EINVAL;
+    cudaSetDevice(ctx->device);
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    double* outs[3] = {pp, ps, illum};
+    for (int k = 0; k < 3; ++k)
+        if (outs[k]) CK(cudaMemcpyAsync(outs[k], ctx->d_stack[k], ni * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (reset)
+        for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->d_stack[k], 0, ni * 8, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (reset) ctx->stacked = false;
+    return OUC_OK;
+}
+
+int ouc_stack_dev(ouc_ctx* ctx, const double** pp, const double** ps, const double** illum) {
+    if (!ctx) return OUC_EINVAL;
+    if (pp) *pp = ctx->d_stack[0];
+    if (ps) *ps = ctx->d_stack[1];
+    if (illum) *illum = ctx->d_stack[2];
+    return OUC_OK;
+}
+
+}  // extern "C"

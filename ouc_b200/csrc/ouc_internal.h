@@ -1,0 +1,123 @@
+// Internal definitions shared by the kernels and the host orchestration.
+//
+// Device layout ("pitched padded grid").  Every cell field lives in its own
+// allocation of (Xc + 2*GX) rows by `pitch` floats:
+//   - Xc = X rounded up to the tile height, Zc = Z rounded up to the tile
+//     width, so a tile never needs a bounds test on its own cells;
+//   - GX guard rows above and below and ZOFF guard columns left of column 0
+//     (and at least ZOFF right of Zc), all zero and never written, so the
+//     halo loads of a tile at the grid edge stay inside the allocation;
+//   - `pitch` is a multiple of 32 floats, so every row starts on a 128-byte
+//     boundary and a float4 at a column multiple of 4 is 16-byte aligned.
+// Field pointers passed to kernels point at cell (0, 0): element (i, j) is
+// f[i * pitch + j] for i in [-GX, Xc+GX) and j in [-ZOFF, Zc+ZOFF).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace ouc {
+
+constexpr int kGX = 16;        // guard rows on each side
+constexpr int kZOFF = 16;      // guard columns on each side
+constexpr int kThreads = 256;  // threads per step CTA
+
+enum Mode : int { kFwd = 0, kRcv = 1, kRec = 2 };
+
+// Boundary ring: the cells within N of the interior edge, on both sides
+// (the reference's four strips of 2N rows/columns, PS:1230-1287, trimmed to
+// the box [L-N, X-L+N) x [L-N, Z-L+N) that the reconstruction reads).
+struct Ring {
+    int L, N, X, Z;
+    int W, H;   // box extent along x and z: nx + 2N, nz + 2N
+    int R;      // ring cells
+    __host__ __device__ static Ring make(int X, int Z, int L, int N) {
+        Ring r;
+        r.L = L; r.N = N; r.X = X; r.Z = Z;
+        r.W = X - 2 * L + 2 * N;
+        r.H = Z - 2 * L + 2 * N;
+        r.R = 4 * N * r.W + 4 * N * (r.H - 4 * N);
+        return r;
+    }
+    // Index of cell (i, j) in the ring, or -1 when the cell is not in it.
+    // Order: top band (j near the top interior edge) W x 2N, bottom band
+    // W x 2N, left band 2N x (H-4N), right band 2N x (H-4N); z contiguous.
+    __host__ __device__ __forceinline__ int index(int i, int j) const {
+        const int ii = i - (L - N), jj = j - (L - N);
+        if (ii < 0 || ii >= W || jj < 0 || jj >= H) return -1;
+        const int n2 = 2 * N;
+        if (jj < n2) return ii * n2 + jj;
+        if (jj >= H - n2) return W * n2 + ii * n2 + (jj - (H - n2));
+        const int hm = H - 2 * n2;
+        if (ii < n2) return 2 * W * n2 + ii * hm + (jj - n2);
+        if (ii >= W - n2) return 2 * W * n2 + n2 * hm + (ii - (W - n2)) * hm + (jj - n2);
+        return -1;
+    }
+    __host__ __device__ __forceinline__ bool in_box(int i, int j) const {
+        return i >= L - N && i < X - L + N && j >= L - N && j < Z - L + N;
+    }
+};
+
+// Strip slot layout: [slot][field][ring cell], fields in the order
+// Ux, Uz, theta, omega, Qzx, Qzz, Qxx, Qxz.
+enum StripField : int { kSUx = 0, kSUz, kSTh, kSOm, kSQzx, kSQzz, kSQxx, kSQxz, kStripFields };
+
+struct StepArgs {
+    int X, Z, pitch, L;
+    int tiles_z, tile_x0, tile_z0;    // tile grid of this launch
+    int t;                            // time step index
+    float a[6];                       // stencil weights a_1..a_N
+    float dx, dz, dt, dt2;
+    // leapfrog state: now (level n, read with halo), past (level n-1, read
+    // at own cells, overwritten with level n+1)
+    const float* __restrict__ now[4];   // Px Pz Sx Sz
+    float* __restrict__ past[4];
+    // S-stage CPML memory, ping-pong: read old (halo), write new (own)
+    const float* __restrict__ f_old[4];  // xx zz xz zx
+    float* __restrict__ f_new[4];
+    // U-stage CPML memory, in place at own cells
+    float* __restrict__ o[8];            // C E B A Tx Tz Wz Wx
+    const float* __restrict__ vp2;
+    const float* __restrict__ vs2;
+    const float* __restrict__ ax;
+    const float* __restrict__ az;
+    // source: theta += wavelet[src_t] at (sx, sz) (kFwd, and kRec when src_recon)
+    int sx, sz, src_t, src_type, src_recon;
+    const float* __restrict__ wavelet;
+    // receivers: row rz; inj_* (kRcv) and rec_* (kFwd) point at row t of a
+    // time-major gather [nt][X]
+    int rz;
+    const float* __restrict__ inj_x;
+    const float* __restrict__ inj_z;
+    float* __restrict__ rec_x;
+    float* __restrict__ rec_z;
+    // boundary strips
+    Ring ring;
+    float* __restrict__ strip_save;         // kFwd: slot t (8 fields) or null
+    const float* __restrict__ strip_u;      // kRec: slot holding U at level t+1
+    const float* __restrict__ strip_s;      // kRec: slot holding theta..Qxz at level t+1
+    // kRec imaging
+    const float* __restrict__ rcv[4];       // receiver Px Pz Sx Sz after this back-step
+    float* __restrict__ acc[3];             // PP, PS, illumination accumulators
+    int img_past;                           // 1: correlate with level t+2 (reference)
+};
+
+struct FinalizeArgs {
+    int X, Z, pitch, L;
+    float dh;
+    const float* acc[3];
+    float* img_pp;     // nx*nz dense, or null
+    float* img_ps;
+    double* stack[3];  // nx*nz dense FP64: PP, PS, illumination (or null)
+};
+
+// Host-side launchers (kernels.cu)
+int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, cudaStream_t s);
+int step_smem_bytes(int N);
+void launch_image_only(const StepArgs& a, cudaStream_t s);
+void launch_finalize(const FinalizeArgs& f, cudaStream_t s);
+void launch_mute(float* gx, float* gz, int X, int nt, int sx, int sz, int rz, int t0, float dt, float dh, float v,
+                 cudaStream_t s);
+void launch_transpose(const float* in, float* out, int rows, int cols, cudaStream_t s);
+void launch_pack_fields(const float* const* f, int nf, int X, int Z, int pitch, float* out, cudaStream_t s);
+
+}  // namespace ouc

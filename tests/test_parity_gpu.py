@@ -1,0 +1,123 @@
+"""GPU parity of the CUDA path (libouc.so, through the C ABI) with the
+reference's outputs (golden fixtures from the reference's own kernels), the
+FP64 oracle and, where built, the reference's kernels compiled for sm_100a.
+
+Tolerances (relative L2 per field):
+  * against the reference's kernels compiled for sm_100a (same hardware,
+    same FMA contraction): 1e-5 after nt steps -- the bar for the FP32 path;
+  * against the golden fixtures, which come from the reference's kernels run
+    on the CPU without FMA contraction: the FP32 round-off floor, measured
+    by the FP64 oracle as ~1e-6 for gathers, ~1e-4 for the separated P/S
+    fields and ~1e-3 for the images -> 1e-5, 5e-4 and 3e-3;
+  * against the FP64 oracle: asserted at the same floors and printed.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ouc_b200 as o
+from helpers import CASES, golden_shot, load_golden, make_context, rel_l2, shot_cfg
+from oracle.oracle import REF_DIR, RefBuild
+
+pytestmark = pytest.mark.gpu
+
+TOL_REF = 1e-5        # vs the reference's sm_100a kernels
+TOL_GATHER = 1e-5     # vs CPU-run reference / FP64 oracle
+TOL_FIELD = 5e-4
+TOL_IMAGE = 3e-3
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_forward_matches_reference(name):
+    g = load_golden(name)
+    with make_context(g) as ctx:
+        gx, gz, _ = ctx.forward(golden_shot(g), g["src"])
+    with make_context(g, nt=int(g["nt_mid"])) as ctx:
+        _, _, f = ctx.forward(golden_shot(g), g["src"][: int(g["nt_mid"])], fields=True)
+    eg = {"gx": rel_l2(gx, g["fwd_gx"]), "gz": rel_l2(gz, g["fwd_gz"])}
+    ef = {n: rel_l2(f[k], g["fwd_fields"][k]) for k, n in enumerate(("Ux", "Uz", "Px", "Pz", "Sx", "Sz"))}
+    print(name, eg, ef)
+    assert max(eg.values()) <= TOL_GATHER, eg
+    assert max(ef.values()) <= TOL_FIELD, ef
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_forward_error_vs_fp64_oracle(oracle, name):
+    g = load_golden(name)
+    sh = shot_cfg(g)
+    gx64, _, _ = oracle.forward(sh, g["vp"], g["vs"], g["ax"], g["az"], g["src"], fp64=True)
+    sh.nt = int(g["nt_mid"])
+    _, _, f64 = oracle.forward(sh, g["vp"], g["vs"], g["ax"], g["az"], g["src"], fp64=True)
+    with make_context(g) as ctx:
+        gx, _, _ = ctx.forward(golden_shot(g), g["src"])
+    with make_context(g, nt=sh.nt) as ctx:
+        _, _, f = ctx.forward(golden_shot(g), g["src"][: sh.nt], fields=True)
+    e = {"gx": rel_l2(gx, gx64), "Px": rel_l2(f[2], f64[2]), "Sx": rel_l2(f[4], f64[4])}
+    print(name, "vs FP64 oracle", e)
+    assert e["gx"] < TOL_GATHER and max(e["Px"], e["Sx"]) < TOL_FIELD
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rtm_matches_reference(name):
+    g = load_golden(name)
+    with make_context(g) as ctx:
+        pp, ps = ctx.rtm_shot(golden_shot(g), g["src"])
+        spp, sps, sil = ctx.stack()
+    errs = {"lap_pp": rel_l2(pp, g["rtm_lap_pp"]), "lap_ps": rel_l2(ps, g["rtm_lap_ps"])}
+    print(name, errs)
+    assert max(errs.values()) <= TOL_IMAGE, errs
+    assert np.allclose(spp, pp.astype(np.float64)) and np.allclose(sps, ps.astype(np.float64))
+    L, X, Z = int(g["L"]), int(g["X"]), int(g["Z"])
+    assert rel_l2(sil, g["rtm_acc"][2][L:X - L, L:Z - L]) < TOL_FIELD
+
+
+@pytest.mark.parametrize("layout", [o.GATHER_XT, o.GATHER_TX])
+def test_rtm_external_records_equal_self_modelled(layout):
+    g = load_golden("g72x56n5")
+    with make_context(g, gather_layout=layout) as ctx:
+        sh = golden_shot(g)
+        gx, gz, _ = ctx.forward(sh, g["src"])
+        pp1, ps1 = ctx.rtm_shot(sh, g["src"], rec=(gx, gz))
+        pp0, ps0 = ctx.rtm_shot(sh, g["src"])
+    assert np.array_equal(pp0, pp1) and np.array_equal(ps0, ps1)
+
+
+def test_forward_deterministic_and_layouts_agree():
+    g = load_golden("g64n6")
+    with make_context(g) as a, make_context(g, gather_layout=o.GATHER_TX) as b:
+        gx1, gz1, _ = a.forward(golden_shot(g), g["src"])
+        gx2, gz2, _ = a.forward(golden_shot(g), g["src"])
+        tx, tz, _ = b.forward(golden_shot(g), g["src"])
+    assert np.array_equal(gx1, gx2) and np.array_equal(gz1, gz2)
+    assert np.array_equal(gx1, tx.T) and np.array_equal(gz1, tz.T)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "libpsref_cuda_g72x56n5.so")),
+                    reason="reference sm_100a build not present")
+@pytest.mark.parametrize("name", ["g64n6", "g72x56n5"])
+def test_matches_reference_cuda_kernels_on_b200(name):
+    """The reference's own kernels compiled for sm_100a on the same inputs."""
+    g = load_golden(name)
+    ref = RefBuild(name, "cuda")
+    dt, dx = np.float32(g["dt"]), np.float32(g["dx"])
+    sx, sz, rz = int(g["sx"]), int(g["sz"]), int(g["rz"])
+    rgx, rgz, rf, _ = ref.forward(sx, sz, rz, dt, dx, dx, g["vp"], g["vs"], g["ax"], g["az"], g["src"], ref.NT)
+    r = ref.rtm(sx, sz, rz, int(g["t0"]), dt, dx, dx, g["vp"], g["vs"], g["ax"], g["az"], g["src"])
+    with make_context(g) as ctx:
+        gx, gz, f = ctx.forward(golden_shot(g), g["src"], fields=True)
+        pp, ps = ctx.rtm_shot(golden_shot(g), g["src"])
+    # fields after the full nt as well as at mid-propagation
+    nm = int(g["nt_mid"])
+    _, _, rfm, _ = ref.forward(sx, sz, rz, dt, dx, dx, g["vp"], g["vs"], g["ax"], g["az"], g["src"], nm)
+    with make_context(g, nt=nm) as ctx:
+        _, _, fm = ctx.forward(golden_shot(g), g["src"][:nm], fields=True)
+    e = {"gx": rel_l2(gx, rgx), "gz": rel_l2(gz, rgz), "lap_pp": rel_l2(pp, r["lap_pp"]),
+         "lap_ps": rel_l2(ps, r["lap_ps"])}
+    for k, n in enumerate(("Ux", "Uz", "Px", "Pz", "Sx", "Sz")):
+        e[n] = rel_l2(f[k], rf[k])
+        e[n + "_mid"] = rel_l2(fm[k], rfm[k])
+    bitexact = {k: bool(np.array_equal(a, b)) for k, a, b in
+                (("gx", gx, rgx), ("fields", f[2:6], rf[2:6]), ("lap_pp", pp, r["lap_pp"]))}
+    print(name, "vs reference CUDA", e, bitexact)
+    assert max(e.values()) <= TOL_REF, e
