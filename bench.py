@@ -173,7 +173,9 @@ def main():
     ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ouc", choices=["ouc", "reference"])
-    ap.add_argument("--nt", type=int, default=4000, help="time steps per shot (the workload's 4000)")
+    ap.add_argument("--nt", type=int, default=None, help="time steps per shot (default: the workload's)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
+                    help="c2: the headline 1000x500 RTM workload; c4: the 4000x1500 grid (HBM-bound profiling)")
     ap.add_argument("--ref-steps", type=int, default=None, help="CPU sample length (time steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -193,7 +195,8 @@ def main():
 
     import ouc_b200 as o
     from ouc_b200 import models
-    w = models.c2(nt=args.nt)
+    make = models.c2 if args.workload == "c2" else models.c4
+    w = make(nt=args.nt) if args.nt else make()
     cfg = w.cfg
     cfg.device = local
     wavelet, t0 = o.ricker(w.fm, cfg.dt, cfg.nt)

@@ -69,7 +69,7 @@ typedef struct ouc_config {
     int half_order;         /* stencil half-width N: 2..6 (PS:16 uses 6)          */
     float dx, dz, dt;       /* spacing (m) and time step (s)                     */
     int nt;                 /* time steps per shot (PS:17)                       */
-    float pml_r;            /* target reflection R of the damping profile (PS:23) */
+    double pml_r;           /* target reflection R of the damping profile (PS:23)  */
     int model_layout;       /* OUC_MODEL_INTERIOR or OUC_MODEL_PADDED            */
     int strip_level;        /* OUC_STRIP_*                                       */
     int image_align;        /* OUC_IMAGE_*                                       */

@@ -17,7 +17,7 @@ OUC_OK, OUC_EINVAL, OUC_ECUDA, OUC_ENOMEM, OUC_EUNSTABLE, OUC_ESTATE, OUC_ETIMEO
 
 class ouc_config(C.Structure):
     _fields_ = [("nx", C.c_int), ("nz", C.c_int), ("npml", C.c_int), ("half_order", C.c_int),
-                ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("nt", C.c_int), ("pml_r", C.c_float),
+                ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("nt", C.c_int), ("pml_r", C.c_double),
                 ("model_layout", C.c_int), ("strip_level", C.c_int), ("image_align", C.c_int),
                 ("strip_precision", C.c_int), ("compensated_image", C.c_int), ("gather_layout", C.c_int),
                 ("device", C.c_int), ("stream", C.c_void_p)]
