@@ -177,6 +177,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
                     help="c2: the headline 1000x500 RTM workload; c4: the 4000x1500 grid (HBM-bound profiling)")
     ap.add_argument("--ref-steps", type=int, default=None, help="CPU sample length (time steps)")
+    ap.add_argument("--batch", type=int, default=8, help="shots advanced together per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -202,32 +203,32 @@ def main():
     wavelet, t0 = o.ricker(w.fm, cfg.dt, cfg.nt)
     X, nt = cfg.X, cfg.nt
 
-    # observed records with the true model (not timed), a few shot positions reused
-    nrec_shots = min(4, len(w.shots))
-    my_shots = [w.shots[(rank + k * world) % len(w.shots)] for k in range(nrec_shots)]
-    for s in my_shots:
-        s.t0 = t0
+    # observed records with the true model (not timed): one record set per
+    # shot of a batch, shot positions spread over the survey
+    B = max(1, args.batch)
+    my_shots = [w.shots[(rank + k * world * max(1, len(w.shots) // (B * world))) % len(w.shots)] for k in range(B)]
+    my_shots = [o.Shot(s.sx, s.sz, s.rz, t0=t0) for s in my_shots]
     true_ctx = o.Context(cfg, w.vp, w.vs, w.rho)
     records = [true_ctx.forward(s, wavelet)[:2] for s in my_shots]
     true_ctx.close()
+    cfg.max_batch = B
     mig = o.Context(cfg, w.vp_mig, w.vs_mig, w.rho)
     stream = torch.cuda.ExternalStream(mig.stream, device=torch.device("cuda", local))
 
     # device-resident inputs
     d_w = torch.from_numpy(wavelet).cuda()
     d_rec = [(torch.from_numpy(r[0]).cuda(), torch.from_numpy(r[1]).cuda()) for r in records]
-    d_img = torch.empty((2, cfg.nx, cfg.nz), dtype=torch.float32, device="cuda")
+    d_img = torch.empty((B, 2, cfg.nx, cfg.nz), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MiB > L2
     torch.cuda.synchronize()
 
-    def shot_dev(k):
-        s = my_shots[k % nrec_shots]
-        rx, rz = d_rec[k % nrec_shots]
-        mig.rtm_shot_dev(s, d_w.data_ptr(), rx.data_ptr(), rz.data_ptr(), d_img[0].data_ptr(), d_img[1].data_ptr())
+    def step_dev():
+        mig.rtm_batch_dev(my_shots, d_w.data_ptr(), [r[0].data_ptr() for r in d_rec], [r[1].data_ptr() for r in d_rec],
+                          [d_img[b, 0].data_ptr() for b in range(B)], [d_img[b, 1].data_ptr() for b in range(B)])
 
     for k in range(args.warmup):
-        shot_dev(k)
-    launches_per_shot = mig.timing()["kernel_launches"]
+        step_dev()
+    launches_per_step = mig.timing()["kernel_launches"]
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -237,9 +238,9 @@ def main():
     bwd_ms = []
     for k in range(args.steps):
         with torch.cuda.stream(stream):
-            flush.fill_(float(k))          # between timed shots: evict L2
+            flush.fill_(float(k))          # between timed steps: evict L2
             ev[k][0].record(stream)
-        shot_dev(k)                        # synchronous on the context stream
+        step_dev()                         # synchronous on the context stream
         with torch.cuda.stream(stream):
             ev[k][1].record(stream)
         t = mig.timing()
@@ -255,18 +256,18 @@ def main():
         dist.all_reduce(stk)   # the cross-shot FP64 stack exchange
         dist.barrier()
     clk = clocks.stop()
-    cells = w.cell_updates_per_shot()
+    cells = w.cell_updates_per_shot() * B
     value = cells * args.steps * world / (ms / 1e3) / 1e9
-    shots_per_hour = 3600.0 * args.steps * world / (ms / 1e3)
+    shots_per_hour = 3600.0 * B * args.steps * world / (ms / 1e3)
 
     # e2e through the host API with pinned buffers
     pin = [(torch.from_numpy(r[0]).pin_memory().numpy(), torch.from_numpy(r[1]).pin_memory().numpy()) for r in records]
     e2e_steps = max(2, args.steps // 2)
-    mig.rtm_shot(my_shots[0], wavelet, rec=pin[0])
+    mig.rtm_batch(my_shots, wavelet, recs=pin)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     for k in range(e2e_steps):
-        mig.rtm_shot(my_shots[k % nrec_shots], wavelet, rec=pin[k % nrec_shots])
+        mig.rtm_batch(my_shots, wavelet, recs=pin)
     e2e_s = time.perf_counter() - t1
     if world > 1:
         tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -277,7 +278,7 @@ def main():
     # roofline of the dominant kernel: the fused forward step (k_step, forward mode)
     peak, peak_kind = measured_peak()
     per_launch_ms = statistics.median(fwd_ms) / nt
-    abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg))
+    abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg)) * B
     achieved = abytes / (per_launch_ms / 1e3) / 1e9
     tr = committed_traffic()
     traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name else None
@@ -292,19 +293,21 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model, modelled records)",
             "config": {"workload": w.name, "grid": [cfg.X, cfg.Z], "interior": [cfg.nx, cfg.nz], "nt": nt,
-                       "half_order": cfg.half_order, "dx_m": cfg.dx, "dt_s": cfg.dt, "step": "one RTM shot",
+                       "half_order": cfg.half_order, "dx_m": cfg.dx, "dt_s": cfg.dt, "step": f"one batch of {B} RTM shots advanced together", "batch": B,
                        "l2": "256 MiB buffer written between timed shots; 3.8 GB of boundary strips per shot",
                        "parallelism": f"shots sharded over {world} GPU(s)"},
             "shots_per_hour": shots_per_hour,
             "phase_ms": {"forward": statistics.median(fwd_ms), "backward": statistics.median(bwd_ms)},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * nt * X * 4 + nt * 4,
-                    "d2h_bytes_per_step": 2 * cfg.nx * cfg.nz * 4, "shots_per_hour": 3600.0 * e2e_steps * world / e2e_s},
-            "roofline": {"kernel": "k_step<5, forward> (fused S+U stage, CPML, strip save)", "bound": "hbm",
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * 2 * nt * X * 4 + nt * 4,
+                    "d2h_bytes_per_step": B * 2 * cfg.nx * cfg.nz * 4,
+                    "shots_per_hour": 3600.0 * B * e2e_steps * world / e2e_s},
+            "roofline": {"kernel": f"k_step<5, forward> (fused S+U stage, CPML, strip save), {B} shots per launch",
+                         "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": abytes,
                          "launch_ms": per_launch_ms, "traffic": traffic},
             "cpu_baseline": cpu,
-            "gpu_launches": int(launches_per_shot * args.steps),
+            "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -78,6 +78,7 @@ typedef struct ouc_config {
     int gather_layout;      /* OUC_GATHER_*                                      */
     int device;             /* CUDA device ordinal                               */
     void* stream;           /* cudaStream_t to run on, or NULL for a private one */
+    int max_batch;          /* shots advanced together per launch (0 or 1: one)  */
 } ouc_config;
 
 typedef struct ouc_shot {
@@ -145,6 +146,18 @@ int ouc_rtm_shot(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const
                  const float* rec_vz, float* img_pp, float* img_ps);
 int ouc_rtm_shot_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, const float* d_rec_vx,
                      const float* d_rec_vz, float* d_img_pp, float* d_img_ps);
+
+/* A batch of RTM shots on the same model, advanced together: every time
+ * step of up to cfg->max_batch shots is one launch per stage (the reference
+ * runs its shots one after another, PS:2108).  Per-shot arrays of pointers;
+ * rec_vx/rec_vz may be NULL (self-modelled records for every shot) and any
+ * img_* entry or array may be NULL.  All images enter the FP64 stack. */
+int ouc_rtm_batch(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const float* wavelet,
+                  const float* const* rec_vx, const float* const* rec_vz, float* const* img_pp,
+                  float* const* img_ps);
+int ouc_rtm_batch_dev(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const float* d_wavelet,
+                      const float* const* d_rec_vx, const float* const* d_rec_vz, float* const* d_img_pp,
+                      float* const* d_img_ps);
 
 /* FP64 cross-shot stack of the Laplacian images (replaces the host FP32 sum
  * through per-shot files, PS:2403-2443) and the FP64 stacked illumination.

@@ -20,7 +20,7 @@ class ouc_config(C.Structure):
                 ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("nt", C.c_int), ("pml_r", C.c_double),
                 ("model_layout", C.c_int), ("strip_level", C.c_int), ("image_align", C.c_int),
                 ("strip_precision", C.c_int), ("compensated_image", C.c_int), ("gather_layout", C.c_int),
-                ("device", C.c_int), ("stream", C.c_void_p)]
+                ("device", C.c_int), ("stream", C.c_void_p), ("max_batch", C.c_int)]
 
 
 class ouc_shot(C.Structure):
@@ -54,6 +54,10 @@ SIGNATURES = {
     "ouc_forward_dev": (C.c_int, [_vp, C.POINTER(ouc_shot), _vp, _vp, _vp]),
     "ouc_rtm_shot": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp, _fp, _fp]),
     "ouc_rtm_shot_dev": (C.c_int, [_vp, C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
+    "ouc_rtm_batch": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), _fp, C.POINTER(_fp), C.POINTER(_fp),
+                                C.POINTER(_fp), C.POINTER(_fp)]),
+    "ouc_rtm_batch_dev": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), _vp, C.POINTER(_vp), C.POINTER(_vp),
+                                    C.POINTER(_vp), C.POINTER(_vp)]),
     "ouc_stack": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
     "ouc_stack_dev": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
 }

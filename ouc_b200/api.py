@@ -43,6 +43,7 @@ class Config:
     gather_layout: int = GATHER_XT
     device: int = 0
     stream: int = 0
+    max_batch: int = 1
 
     def c(self):
         c = _lib.ouc_config()
@@ -187,6 +188,43 @@ class Context:
         """Device-pointer variant (integers); no host copies."""
         sc = shot.c()
         check(lib().ouc_rtm_shot_dev(self._h, C.byref(sc), d_wavelet, d_rec_vx, d_rec_vz, d_img_pp, d_img_ps),
+              self._h)
+
+    def rtm_batch(self, shots, wavelet, recs=None):
+        """RTM of several shots advanced together (up to cfg.max_batch per
+        launch); recs = list of (rec_vx, rec_vz) or None.  Returns a list of
+        (img_pp, img_ps)."""
+        n = len(shots)
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        sh = (_lib.ouc_shot * n)(*[s.c() for s in shots])
+        FP = C.POINTER(C.c_float)
+        keep = []
+        rx = rz = None
+        if recs is not None:
+            ax_ = [_f32(r[0]) for r in recs]
+            az_ = [_f32(r[1]) for r in recs]
+            for a_ in ax_ + az_:
+                assert a_.shape == self._gshape()
+            keep += ax_ + az_
+            rx = (FP * n)(*[_p(a_) for a_ in ax_])
+            rz = (FP * n)(*[_p(a_) for a_ in az_])
+        imgs = [(np.zeros((self.cfg.nx, self.cfg.nz), np.float32), np.zeros((self.cfg.nx, self.cfg.nz), np.float32))
+                for _ in range(n)]
+        ipp = (FP * n)(*[_p(i[0]) for i in imgs])
+        ips = (FP * n)(*[_p(i[1]) for i in imgs])
+        check(lib().ouc_rtm_batch(self._h, n, sh, _p(w), rx, rz, ipp, ips), self._h)
+        return imgs
+
+    def rtm_batch_dev(self, shots, d_wavelet, d_rx=None, d_rz=None, d_ipp=None, d_ips=None):
+        """Device-pointer variant: lists of device addresses (integers)."""
+        n = len(shots)
+        sh = (_lib.ouc_shot * n)(*[s.c() for s in shots])
+        VP = C.c_void_p
+
+        def arr(xs):
+            return None if xs is None else (VP * n)(*xs)
+        check(lib().ouc_rtm_batch_dev(self._h, n, sh, d_wavelet, arr(d_rx), arr(d_rz), arr(d_ipp), arr(d_ips)),
               self._h)
 
     def forward_dev(self, shot: Shot, d_wavelet, d_gx=None, d_gz=None):

@@ -5,6 +5,9 @@
 // forward loop with boundary-strip save, the mute, the backward loop that
 // back-propagates the records and reconstructs the source wavefield, the
 // imaging condition and the per-shot image finalisation with an FP64 stack.
+// Shots of a batch advance together: each time step is one launch per stage
+// with blockIdx.y selecting the shot (the reference runs shots one after the
+// other, PS:2108).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,14 +38,16 @@ const double kWeights[7][6] = {
     {1.2213364, -9.6931458e-2, 1.7447662e-2, -2.9672895e-3, 3.5900540e-4, -2.1847812e-5},
 };
 
+constexpr int kFieldsPerSide = 24;                    // now 4, past 4, F old 4, F new 4, O 8
+constexpr int kFieldsPerShot = 2 * kFieldsPerSide + 3;   // source side, receiver side, accumulators
+
+// Field pointers of one wavefield (shot 0 of the batch).
 struct Side {
     float* now[4];
     float* past[4];
     float* fo[4];
     float* fn[4];
     float* o[8];
-    float* base;      // first field of the side (for zeroing)
-    size_t floats;    // span of the side's fields
     void swap_levels() { for (int k = 0; k < 4; ++k) std::swap(now[k], past[k]); }
     void swap_memory() { for (int k = 0; k < 4; ++k) std::swap(fo[k], fn[k]); }
 };
@@ -53,7 +58,9 @@ struct ouc_ctx {
     ouc_config cfg;
     int X = 0, Z = 0, L = 0, N = 0, nx = 0, nz = 0, nt = 0;
     int Xc = 0, Zc = 0, pitch = 0;
+    int batch = 1;               // shots per launch
     size_t fstride = 0;          // floats per field allocation
+    size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;
     int rec_tx0 = 0, rec_tz0 = 0, rec_tiles_x = 0, rec_tiles_z = 0;
     float a[6] = {0, 0, 0, 0, 0, 0};
@@ -66,23 +73,24 @@ struct ouc_ctx {
     std::vector<float> vp_host;  // padded Vp (for the mute's velocity)
 
     // device memory
-    float* arena = nullptr;
-    size_t arena_floats = 0;
+    float* model = nullptr;      // 4 fields: vp2 vs2 ax az
+    float* state = nullptr;      // batch shot blocks
     float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
     Side src{}, rcv{};
     float* acc[3] = {nullptr, nullptr, nullptr};
-    float* gather[2] = {nullptr, nullptr};    // time-major [nt][X]
-    float* staging = nullptr;                  // 2*nt*X floats for transposes / packing
+    float* gathers = nullptr;    // [batch][2][nt][X], time-major
+    float* staging = nullptr;    // max(nt*X, 4*X*Z) floats for transposes / packing
     float* d_wavelet = nullptr;
-    float* d_img[2] = {nullptr, nullptr};
+    float* d_img = nullptr;      // [batch][2][nx][nz]
     double* d_stack[3] = {nullptr, nullptr, nullptr};
-    float* strips = nullptr;
-    size_t strip_slot = 0;                     // floats per slot
+    float* strips = nullptr;     // [batch][nt][8][R]
+    size_t strip_slot = 0;       // floats per slot
+    ShotDesc* d_desc = nullptr;  // [batch]
     size_t bytes = 0;
-    bool stacked = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
-    float* field(size_t k) const { return arena + k * fstride + (size_t)kGX * pitch + kZOFF; }
+    float* field(float* base, size_t k) const { return base + k * fstride + (size_t)kGX * pitch + kZOFF; }
+    float* gather(int b, int comp) const { return gathers + ((size_t)b * 2 + comp) * (size_t)nt * X; }
 };
 
 namespace {
@@ -157,8 +165,13 @@ StepArgs base_args(const ouc_ctx* c) {
     for (int k = 0; k < 6; ++k) a.a[k] = c->a[k];
     a.dx = c->cfg.dx; a.dz = c->cfg.dz; a.dt = c->cfg.dt;
     a.dt2 = c->cfg.dt * c->cfg.dt;
+    a.rdx = 1.0f / c->cfg.dx;   // correctly rounded reciprocal (host IEEE division)
+    a.rdz = 1.0f / c->cfg.dz;
     a.vp2 = c->vp2; a.vs2 = c->vs2; a.ax = c->ax; a.az = c->az;
+    a.shot_stride = c->shot_stride;
+    a.strip_slot = c->strip_slot;
     a.ring = c->ring;
+    a.shots = c->d_desc;
     return a;
 }
 
@@ -182,8 +195,7 @@ int check_shot(ouc_ctx* ctx, const ouc_shot* s) {
 
 int ensure_strips(ouc_ctx* ctx) {
     if (ctx->strips) return OUC_OK;
-    ctx->strip_slot = (size_t)kStripFields * ctx->ring.R;
-    size_t bytes = ctx->strip_slot * (size_t)ctx->nt * sizeof(float);
+    const size_t bytes = ctx->strip_slot * (size_t)ctx->nt * ctx->batch * sizeof(float);
     cudaError_t e = cudaMalloc(&ctx->strips, bytes);
     if (e != cudaSuccess) {
         ctx->strips = nullptr;
@@ -194,59 +206,78 @@ int ensure_strips(ouc_ctx* ctx) {
     return OUC_OK;
 }
 
-// Forward time loop (PS:2258-2292).  Records into the time-major gathers when
-// `record`, saves the boundary ring of every step when `save`.
-int run_forward(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, bool record, bool save) {
-    Side& s = ctx->src;
-    CK(cudaMemsetAsync(s.base, 0, s.floats * sizeof(float), ctx->stream));
+// Upload the descriptors of n shots (padded coordinates).
+int upload_desc(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_wavelet) {
+    std::vector<ShotDesc> d(n);
+    for (int b = 0; b < n; ++b) {
+        d[b].sx = shots[b].sx + ctx->L;
+        d[b].sz = shots[b].sz + ctx->L;
+        d[b].rz = shots[b].rz + ctx->L;
+        d[b].src_type = shots[b].src_type;
+        d[b].wavelet = d_wavelet;
+        d[b].gather_x = ctx->gather(b, 0);
+        d[b].gather_z = ctx->gather(b, 1);
+        d[b].strips = ctx->strips ? ctx->strips + (size_t)b * ctx->nt * ctx->strip_slot : nullptr;
+    }
+    CK(cudaMemcpyAsync(ctx->d_desc, d.data(), n * sizeof(ShotDesc), cudaMemcpyHostToDevice, ctx->stream));
+    return OUC_OK;
+}
+
+// Zero the source- or receiver-side fields (and optionally the accumulators)
+// of n shots.
+int zero_side(ouc_ctx* ctx, int n, int side, bool with_acc) {
+    for (int b = 0; b < n; ++b) {
+        float* base = ctx->state + (size_t)b * ctx->shot_stride + (size_t)side * kFieldsPerSide * ctx->fstride;
+        CK(cudaMemsetAsync(base, 0, (size_t)kFieldsPerSide * ctx->fstride * sizeof(float), ctx->stream));
+        if (with_acc) {
+            float* acc = ctx->state + (size_t)b * ctx->shot_stride + (size_t)2 * kFieldsPerSide * ctx->fstride;
+            CK(cudaMemsetAsync(acc, 0, (size_t)3 * ctx->fstride * sizeof(float), ctx->stream));
+        }
+    }
+    return OUC_OK;
+}
+
+// Forward time loop (PS:2258-2292) of n shots.  Records into the time-major
+// gathers when `record`, saves the boundary ring of every step when `save`.
+int run_forward(ouc_ctx* ctx, int n, bool record, bool save) {
+    Side s = ctx->src;
+    int rc = zero_side(ctx, n, 0, false);
+    if (rc) return rc;
     StepArgs a = base_args(ctx);
-    a.sx = shot->sx + ctx->L; a.sz = shot->sz + ctx->L;
-    a.src_type = shot->src_type;
-    a.wavelet = d_wavelet;
-    a.rz = shot->rz + ctx->L;
+    a.record = record;
+    a.save = save;
     for (int t = 0; t < ctx->nt; ++t) {
         bind_side(a, s);
-        a.t = t; a.src_t = t;
-        a.rec_x = record ? ctx->gather[0] + (size_t)t * ctx->X : nullptr;
-        a.rec_z = record ? ctx->gather[1] + (size_t)t * ctx->X : nullptr;
-        a.strip_save = save ? ctx->strips + (size_t)t * ctx->strip_slot : nullptr;
-        if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+        a.t = t;
+        if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
         s.swap_levels();
         s.swap_memory();
     }
+    ctx->src = s;
     ctx->timing.kernel_launches += ctx->nt;
     CK(cudaGetLastError());
     return OUC_OK;
 }
 
-// Backward loop (PS:2313-2364) and imaging; the source-side state holds the
-// forward's last two levels on entry.
-int run_backward(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet) {
-    Side& s = ctx->src;
-    Side& r = ctx->rcv;
+// Backward loop (PS:2313-2364) and imaging of n shots; the source side
+// holds the forward's last two levels on entry.
+int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
+    Side s = ctx->src;
+    Side r = ctx->rcv;
     const int nt = ctx->nt;
-    CK(cudaMemsetAsync(r.base, 0, r.floats * sizeof(float), ctx->stream));
-    for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->acc[k] - (size_t)kGX * ctx->pitch - kZOFF, 0,
-                                                   ctx->fstride * sizeof(float), ctx->stream));
+    int rc = zero_side(ctx, n, 1, true);
+    if (rc) return rc;
     StepArgs ar = base_args(ctx);
-    ar.rz = shot->rz + ctx->L;
     StepArgs as = base_args(ctx);
     as.tiles_z = ctx->rec_tiles_z; as.tile_x0 = ctx->rec_tx0; as.tile_z0 = ctx->rec_tz0;
-    as.sx = shot->sx + ctx->L; as.sz = shot->sz + ctx->L;
-    as.wavelet = d_wavelet;
     as.img_past = ctx->cfg.image_align == OUC_IMAGE_REFERENCE;
     for (int k = 0; k < 3; ++k) as.acc[k] = ctx->acc[k];
-    const bool exact = ctx->cfg.strip_level == OUC_STRIP_EXACT;
-    // theta-type source only: a force source does not enter the S-stage
-    const bool theta_src = shot->src_type == OUC_SRC_THETA;
     long long launches = 0;
     for (int t = nt - 1; t >= 0; --t) {
         // receiver side: injection + S/U stages with damping (PS:2319-2324, 2349-2354)
         bind_side(ar, r);
         ar.t = t;
-        ar.inj_x = ctx->gather[0] + (size_t)t * ctx->X;
-        ar.inj_z = ctx->gather[1] + (size_t)t * ctx->X;
-        if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+        if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
         r.swap_levels();
         r.swap_memory();
         ++launches;
@@ -255,21 +286,19 @@ int run_backward(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet) {
             StepArgs ai = base_args(ctx);
             for (int k = 0; k < 4; ++k) { ai.now[k] = s.now[k]; ai.rcv[k] = r.now[k]; }
             for (int k = 0; k < 3; ++k) ai.acc[k] = ctx->acc[k];
-            launch_image_only(ai, ctx->stream);
+            launch_image_only(ai, n, ctx->stream);
             ++launches;
             s.swap_levels();   // now = level NT-1, past = level NT
             continue;
         }
-        // source side: inverse leapfrog on the interior from level t+1 and t+2
+        // source side: inverse leapfrog on the interior from levels t+1 and t+2
         bind_side(as, s);
         as.t = t;
-        as.src_t = t + 1;
-        as.src_recon = theta_src && (exact || t + 1 == nt - 1);
-        const int slot_u = exact ? t : (t + 1 == nt - 1 ? nt - 2 : t + 1);
-        as.strip_u = ctx->strips + (size_t)slot_u * ctx->strip_slot;
-        as.strip_s = ctx->strips + (size_t)(t + 1) * ctx->strip_slot;
+        as.src_recon = theta_src && (exact_strips || t + 1 == nt - 1);
+        as.slot_u = exact_strips ? t : (t + 1 == nt - 1 ? nt - 2 : t + 1);
+        as.slot_s = t + 1;
         for (int k = 0; k < 4; ++k) as.rcv[k] = r.now[k];
-        if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+        if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
         s.swap_levels();
         ++launches;
     }
@@ -278,15 +307,16 @@ int run_backward(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet) {
     return OUC_OK;
 }
 
-int finalize(ouc_ctx* ctx, float* d_pp, float* d_ps) {
+int finalize(ouc_ctx* ctx, int n) {
     FinalizeArgs f;
     f.X = ctx->X; f.Z = ctx->Z; f.pitch = ctx->pitch; f.L = ctx->L;
+    f.nshots = n;
+    f.shot_stride = ctx->shot_stride;
     f.dh = ctx->cfg.dx;   // main() passes dx as the Laplacian spacing (PS:2372)
     for (int k = 0; k < 3; ++k) { f.acc[k] = ctx->acc[k]; f.stack[k] = ctx->d_stack[k]; }
-    f.img_pp = d_pp; f.img_ps = d_ps;
+    f.img = ctx->d_img;
     launch_finalize(f, ctx->stream);
     ctx->timing.kernel_launches += 1;
-    ctx->stacked = true;
     CK(cudaGetLastError());
     return OUC_OK;
 }
@@ -322,6 +352,12 @@ int gather_out(ouc_ctx* ctx, const float* src_tx, float* dst, bool host) {
     }
     CK(cudaMemcpyAsync(dst, from, n * 4, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
     return OUC_OK;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
 }
 
 }  // namespace
@@ -375,14 +411,23 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     if (!ctx) return OUC_ENOMEM;
     ctx->cfg = *cfg;
     const int N = cfg->half_order, L = cfg->npml;
-    auto bad = [&](const char* m) { ctx->err = m; int rc = OUC_EINVAL; ouc_destroy(ctx); return rc; };
-    if (N != 2 && N != 4 && N != 5 && N != 6) return bad("half_order must be 2, 4, 5 or 6");
+    auto bad = [&](const std::string& m, int code = OUC_EINVAL) {
+        ctx->err = m;
+        ouc_destroy(ctx);
+        return code;
+    };
+    if (N != 2 && N != 5 && N != 6) return bad("half_order must be 2, 5 or 6");
     if (cfg->nx < 4 * N || cfg->nz < 4 * N) return bad("interior must be at least 4N cells in each direction");
     if (L < N) return bad("npml must be at least the stencil half-width");
     if (!(cfg->dx > 0) || !(cfg->dz > 0) || !(cfg->dt > 0) || cfg->nt < 2) return bad("bad spacing, time step or nt");
+    // the corrected-reciprocal division is exact for quotients above 2^-120,
+    // which the 2^-112 accumulator guard ensures for spacings up to 256
+    if (cfg->dx > 256.f || cfg->dz > 256.f) return bad("grid spacing above 256 is not supported");
     if (!(cfg->pml_r > 0 && cfg->pml_r < 1)) return bad("pml_r must be in (0, 1)");
+    if (cfg->max_batch < 0 || cfg->max_batch > 256) return bad("max_batch must be in [0, 256]");
     ctx->N = N; ctx->L = L; ctx->nx = cfg->nx; ctx->nz = cfg->nz; ctx->nt = cfg->nt;
     ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
+    ctx->batch = std::max(1, cfg->max_batch);
     for (int k = 0; k < N; ++k) ctx->a[k] = (float)kWeights[N][k];
     const int X = ctx->X, Z = ctx->Z;
 
@@ -411,11 +456,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     double sa = 0;
     for (int k = 0; k < N; ++k) sa += fabs(kWeights[N][k]);
     const double cfl = cfg->dt * vmax * sa * sqrt(1.0 / (cfg->dx * cfg->dx) + 1.0 / (cfg->dz * cfg->dz));
-    if (cfl > 1.0) {
-        ctx->err = "CFL number " + std::to_string(cfl) + " > 1 for this dt";
-        ouc_destroy(ctx);
-        return OUC_EUNSTABLE;
-    }
+    if (cfl > 1.0) return bad("CFL number " + std::to_string(cfl) + " > 1 for this dt", OUC_EUNSTABLE);
     std::vector<float> hax((size_t)X * Z), haz((size_t)X * Z);
     damping(P_vp, X, Z, L, cfg->pml_r, hax, haz);
     ctx->vp_host = P_vp;
@@ -426,25 +467,18 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0) {
         cudaGetLastError();
-        ctx->err = "no CUDA device";
-        ouc_destroy(ctx);
-        return OUC_ENODEV;
+        return bad("no CUDA device", OUC_ENODEV);
     }
     ctx->device = cfg->device;
-    if (cudaSetDevice(ctx->device) != cudaSuccess) { ctx->err = "cudaSetDevice failed"; ouc_destroy(ctx); return OUC_ENODEV; }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return bad("cudaSetDevice failed", OUC_ENODEV);
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, ctx->device);
-    if (prop.major != 10) {
-        ctx->err = std::string("device ") + prop.name + " is not sm_100";
-        ouc_destroy(ctx);
-        return OUC_ENODEV;
-    }
+    if (prop.major != 10) return bad(std::string("device ") + prop.name + " is not sm_100", OUC_ENODEV);
     if (cfg->stream) {
         ctx->stream = (cudaStream_t)cfg->stream;
     } else {
-        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-            ctx->err = "cannot create stream"; ouc_destroy(ctx); return OUC_ECUDA;
-        }
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bad("cannot create stream", OUC_ECUDA);
         ctx->own_stream = true;
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
@@ -455,63 +489,55 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->Xc = ctx->tiles_x * TX; ctx->Zc = ctx->tiles_z * TZ;
     ctx->pitch = ((kZOFF + ctx->Zc + kZOFF) + 31) / 32 * 32;
     ctx->fstride = (size_t)(ctx->Xc + 2 * kGX) * ctx->pitch;
+    ctx->shot_stride = (size_t)kFieldsPerShot * ctx->fstride;
     ctx->rec_tx0 = L / TX; ctx->rec_tz0 = L / TZ;
     ctx->rec_tiles_x = (X - L - 1) / TX - ctx->rec_tx0 + 1;
     ctx->rec_tiles_z = (Z - L - 1) / TZ - ctx->rec_tz0 + 1;
     ctx->ring = Ring::make(X, Z, L, N);
+    ctx->strip_slot = (size_t)kStripFields * ctx->ring.R;
 
-    // fields: model 4, source side 24, receiver side 24, accumulators 3
-    const int nfields = 4 + 24 + 24 + 3;
-    ctx->arena_floats = ctx->fstride * nfields;
-    size_t arena_bytes = ctx->arena_floats * sizeof(float);
-    if (cudaMalloc(&ctx->arena, arena_bytes) != cudaSuccess) {
-        cudaGetLastError();
-        ctx->err = "cannot allocate wavefield state";
-        ouc_destroy(ctx);
-        return OUC_ENOMEM;
-    }
-    ctx->bytes += arena_bytes;
-    cudaMemsetAsync(ctx->arena, 0, arena_bytes, ctx->stream);
-    size_t k = 0;
-    ctx->vp2 = ctx->field(k++); ctx->vs2 = ctx->field(k++); ctx->ax = ctx->field(k++); ctx->az = ctx->field(k++);
-    for (Side* s : {&ctx->src, &ctx->rcv}) {
-        s->base = ctx->arena + k * ctx->fstride;
-        s->floats = 24 * ctx->fstride;
-        for (int q = 0; q < 4; ++q) s->now[q] = ctx->field(k++);
-        for (int q = 0; q < 4; ++q) s->past[q] = ctx->field(k++);
-        for (int q = 0; q < 4; ++q) s->fo[q] = ctx->field(k++);
-        for (int q = 0; q < 4; ++q) s->fn[q] = ctx->field(k++);
-        for (int q = 0; q < 8; ++q) s->o[q] = ctx->field(k++);
-    }
-    for (int q = 0; q < 3; ++q) ctx->acc[q] = ctx->field(k++);
-
+    const size_t model_bytes = 4 * ctx->fstride * sizeof(float);
+    const size_t state_bytes = ctx->shot_stride * ctx->batch * sizeof(float);
     const size_t ng = (size_t)ctx->nt * X;
     const size_t ni = (size_t)ctx->nx * ctx->nz;
-    bool ok = cudaMalloc(&ctx->gather[0], ng * 4) == cudaSuccess && cudaMalloc(&ctx->gather[1], ng * 4) == cudaSuccess &&
-              cudaMalloc(&ctx->staging, std::max(ng, (size_t)6 * X * Z) * 4) == cudaSuccess &&
+    const size_t stage = std::max(ng, (size_t)4 * X * Z);
+    bool ok = cudaMalloc(&ctx->model, model_bytes) == cudaSuccess &&
+              cudaMalloc(&ctx->state, state_bytes) == cudaSuccess &&
+              cudaMalloc(&ctx->gathers, 2 * ng * ctx->batch * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->staging, stage * 4) == cudaSuccess &&
               cudaMalloc(&ctx->d_wavelet, (size_t)ctx->nt * 4) == cudaSuccess &&
-              cudaMalloc(&ctx->d_img[0], ni * 4) == cudaSuccess && cudaMalloc(&ctx->d_img[1], ni * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->d_img, 2 * ni * ctx->batch * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->d_desc, ctx->batch * sizeof(ShotDesc)) == cudaSuccess &&
               cudaMalloc(&ctx->d_stack[0], ni * 8) == cudaSuccess && cudaMalloc(&ctx->d_stack[1], ni * 8) == cudaSuccess &&
               cudaMalloc(&ctx->d_stack[2], ni * 8) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
-        ctx->err = "cannot allocate gathers, images or stack";
-        ouc_destroy(ctx);
-        return OUC_ENOMEM;
+        return bad("cannot allocate wavefield state, gathers, images or stack", OUC_ENOMEM);
     }
-    ctx->bytes += 2 * ng * 4 + std::max(ng, (size_t)6 * X * Z) * 4 + (size_t)ctx->nt * 4 + 2 * ni * 4 + 3 * ni * 8;
+    ctx->bytes += model_bytes + state_bytes + 2 * ng * ctx->batch * 4 + stage * 4 + (size_t)ctx->nt * 4 +
+                  2 * ni * ctx->batch * 4 + 3 * ni * 8;
+    // guards and padding of every field must stay zero: clear everything once
+    cudaMemsetAsync(ctx->model, 0, model_bytes, ctx->stream);
+    cudaMemsetAsync(ctx->state, 0, state_bytes, ctx->stream);
     for (int q = 0; q < 3; ++q) cudaMemsetAsync(ctx->d_stack[q], 0, ni * 8, ctx->stream);
+    ctx->vp2 = ctx->field(ctx->model, 0); ctx->vs2 = ctx->field(ctx->model, 1);
+    ctx->ax = ctx->field(ctx->model, 2); ctx->az = ctx->field(ctx->model, 3);
+    size_t k = 0;
+    for (Side* s : {&ctx->src, &ctx->rcv}) {
+        for (int q = 0; q < 4; ++q) s->now[q] = ctx->field(ctx->state, k++);
+        for (int q = 0; q < 4; ++q) s->past[q] = ctx->field(ctx->state, k++);
+        for (int q = 0; q < 4; ++q) s->fo[q] = ctx->field(ctx->state, k++);
+        for (int q = 0; q < 4; ++q) s->fn[q] = ctx->field(ctx->state, k++);
+        for (int q = 0; q < 8; ++q) s->o[q] = ctx->field(ctx->state, k++);
+    }
+    for (int q = 0; q < 3; ++q) ctx->acc[q] = ctx->field(ctx->state, k++);
     int rc = OUC_OK;
     if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
         (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data()))) {
         ouc_destroy(ctx);
         return rc;
     }
-    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
-        ctx->err = "setup failed";
-        ouc_destroy(ctx);
-        return OUC_ECUDA;
-    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return bad("setup failed", OUC_ECUDA);
     *out = ctx;
     return OUC_OK;
 }
@@ -519,10 +545,9 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
 int ouc_destroy(ouc_ctx* ctx) {
     if (!ctx) return OUC_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    cudaFree(ctx->arena);
-    cudaFree(ctx->gather[0]); cudaFree(ctx->gather[1]);
-    cudaFree(ctx->staging); cudaFree(ctx->d_wavelet);
-    cudaFree(ctx->d_img[0]); cudaFree(ctx->d_img[1]);
+    cudaFree(ctx->model); cudaFree(ctx->state);
+    cudaFree(ctx->gathers); cudaFree(ctx->staging); cudaFree(ctx->d_wavelet);
+    cudaFree(ctx->d_img); cudaFree(ctx->d_desc);
     for (auto* p : ctx->d_stack) cudaFree(p);
     cudaFree(ctx->strips);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
@@ -562,11 +587,12 @@ static int forward_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet
         CK(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
         d_w = ctx->d_wavelet;
     }
+    if ((rc = upload_desc(ctx, 1, shot, d_w))) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    if ((rc = run_forward(ctx, shot, d_w, gx || gz, false))) return rc;
+    if ((rc = run_forward(ctx, 1, gx || gz, false))) return rc;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    if (gx && (rc = gather_out(ctx, ctx->gather[0], gx, host))) return rc;
-    if (gz && (rc = gather_out(ctx, ctx->gather[1], gz, host))) return rc;
+    if (gx && (rc = gather_out(ctx, ctx->gather(0, 0), gx, host))) return rc;
+    if (gz && (rc = gather_out(ctx, ctx->gather(0, 1), gz, host))) return rc;
     if (fields && host) {
         const float* f[4] = {ctx->src.now[0], ctx->src.now[1], ctx->src.now[2], ctx->src.now[3]};
         launch_pack_fields(f, 4, ctx->X, ctx->Z, ctx->pitch, ctx->staging, ctx->stream);
@@ -582,12 +608,8 @@ static int forward_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet
             fields[C + k] = fields[3 * C + k] + fields[5 * C + k];   // Uz = Pz + Sz
         }
     }
-    float a = 0, b = 0, c = 0;
-    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-    cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
-    ctx->timing.forward_ms = b;
-    ctx->timing.copy_ms = a + c;
+    ctx->timing.forward_ms = elapsed(ctx->ev[1], ctx->ev[2]);
+    ctx->timing.copy_ms = elapsed(ctx->ev[0], ctx->ev[1]) + elapsed(ctx->ev[2], ctx->ev[3]);
     return OUC_OK;
 }
 
@@ -599,67 +621,94 @@ int ouc_forward_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, 
     return forward_impl(ctx, shot, d_wavelet, d_gx, d_gz, nullptr, false);
 }
 
-static int rtm_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rx, const float* rz,
-                    float* img_pp, float* img_ps, bool host) {
+// One group of n <= batch shots.
+static int rtm_group(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_w, const float* const* rx,
+                     const float* const* rz, float* const* ipp, float* const* ips, bool host) {
+    int rc;
+    const bool self_records = rx == nullptr;
+    if ((rc = upload_desc(ctx, n, shots, d_w))) return rc;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    if ((rc = run_forward(ctx, n, self_records, true))) return rc;
+    for (int b = 0; b < n && !self_records; ++b) {
+        if (!rx[b] || !rz[b]) return fail(ctx, OUC_EINVAL, "record pointer missing for a shot");
+        if ((rc = gather_in(ctx, rx[b], ctx->gather(b, 0), host))) return rc;
+        if ((rc = gather_in(ctx, rz[b], ctx->gather(b, 1), host))) return rc;
+    }
+    for (int b = 0; b < n; ++b) {
+        if (!shots[b].mute) continue;
+        const int sx = shots[b].sx + ctx->L, sz = shots[b].sz + ctx->L, rzz = shots[b].rz + ctx->L;
+        const float v = ctx->vp_host[(size_t)sx * ctx->Z + rzz];   // Vp at (Sx, Z_receive), PS:1645
+        launch_mute(ctx->gather(b, 0), ctx->gather(b, 1), ctx->X, ctx->nt, sx, sz, rzz, shots[b].t0, ctx->cfg.dt,
+                    ctx->cfg.dx, v, ctx->stream);
+        ctx->timing.kernel_launches += 1;
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    const bool theta = shots[0].src_type == OUC_SRC_THETA;
+    for (int b = 1; b < n; ++b)
+        if ((shots[b].src_type == OUC_SRC_THETA) != theta) return fail(ctx, OUC_EINVAL, "mixed source types in a batch");
+    if ((rc = run_backward(ctx, n, ctx->cfg.strip_level == OUC_STRIP_EXACT, theta))) return rc;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    if ((rc = finalize(ctx, n))) return rc;
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    const cudaMemcpyKind kind = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    for (int b = 0; b < n; ++b) {
+        if (ipp && ipp[b]) CK(cudaMemcpyAsync(ipp[b], ctx->d_img + (size_t)(2 * b) * ni, ni * 4, kind, ctx->stream));
+        if (ips && ips[b]) CK(cudaMemcpyAsync(ips[b], ctx->d_img + (size_t)(2 * b + 1) * ni, ni * 4, kind, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->timing.forward_ms += elapsed(ctx->ev[0], ctx->ev[1]);
+    ctx->timing.backward_ms += elapsed(ctx->ev[1], ctx->ev[2]);
+    ctx->timing.finalize_ms += elapsed(ctx->ev[2], ctx->ev[3]);
+    return OUC_OK;
+}
+
+static int rtm_batch_impl(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const float* wavelet,
+                          const float* const* rx, const float* const* rz, float* const* ipp, float* const* ips,
+                          bool host) {
     if (!ctx) return OUC_EINVAL;
-    int rc = check_shot(ctx, shot);
-    if (rc) return rc;
+    if (nshots < 1 || !shots) return fail(ctx, OUC_EINVAL, "no shots");
     if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
     if ((rx == nullptr) != (rz == nullptr)) return fail(ctx, OUC_EINVAL, "give both record components or neither");
+    int rc;
+    for (int b = 0; b < nshots; ++b)
+        if ((rc = check_shot(ctx, &shots[b]))) return rc;
     cudaSetDevice(ctx->device);
     if ((rc = ensure_strips(ctx))) return rc;
     ctx->timing = ouc_timing{};
     const float* d_w = wavelet;
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     if (host) {
         CK(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
         d_w = ctx->d_wavelet;
     }
-    if ((rc = run_forward(ctx, shot, d_w, rx == nullptr, true))) return rc;
-    if (rx) {
-        if ((rc = gather_in(ctx, rx, ctx->gather[0], host))) return rc;
-        if ((rc = gather_in(ctx, rz, ctx->gather[1], host))) return rc;
+    for (int s0 = 0; s0 < nshots; s0 += ctx->batch) {
+        const int n = std::min(ctx->batch, nshots - s0);
+        rc = rtm_group(ctx, n, shots + s0, d_w, rx ? rx + s0 : nullptr, rz ? rz + s0 : nullptr, ipp ? ipp + s0 : nullptr,
+                       ips ? ips + s0 : nullptr, host);
+        if (rc) return rc;
     }
-    if (shot->mute) {
-        const int sx = shot->sx + ctx->L, sz = shot->sz + ctx->L, rzz = shot->rz + ctx->L;
-        const float v = ctx->vp_host[(size_t)sx * ctx->Z + rzz];   // Vp at (Sx, Z_receive), PS:1645
-        launch_mute(ctx->gather[0], ctx->gather[1], ctx->X, ctx->nt, sx, sz, rzz, shot->t0, ctx->cfg.dt, ctx->cfg.dx, v,
-                    ctx->stream);
-        ctx->timing.kernel_launches += 1;
-    }
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    if ((rc = run_backward(ctx, shot, d_w))) return rc;
-    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    float* d_pp = host ? ctx->d_img[0] : img_pp;
-    float* d_ps = host ? ctx->d_img[1] : img_ps;
-    if ((rc = finalize(ctx, d_pp, d_ps))) return rc;
-    const size_t ni = (size_t)ctx->nx * ctx->nz;
-    if (host && img_pp) CK(cudaMemcpyAsync(img_pp, d_pp, ni * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (host && img_ps) CK(cudaMemcpyAsync(img_ps, d_ps, ni * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    float a = 0, b = 0, c = 0;
-    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-    cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
-    ctx->timing.forward_ms = a;
-    ctx->timing.backward_ms = b;
-    ctx->timing.finalize_ms = c;
     return OUC_OK;
 }
 
 int ouc_rtm_shot(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rx, const float* rz,
                  float* img_pp, float* img_ps) {
-    return rtm_impl(ctx, shot, wavelet, rx, rz, img_pp, img_ps, true);
+    return rtm_batch_impl(ctx, 1, shot, wavelet, rx ? &rx : nullptr, rz ? &rz : nullptr, &img_pp, &img_ps, true);
 }
 
 int ouc_rtm_shot_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, const float* d_rx, const float* d_rz,
                      float* d_img_pp, float* d_img_ps) {
-    if (ctx && (!d_img_pp || !d_img_ps)) {
-        d_img_pp = d_img_pp ? d_img_pp : ctx->d_img[0];
-        d_img_ps = d_img_ps ? d_img_ps : ctx->d_img[1];
-    }
-    return rtm_impl(ctx, shot, d_wavelet, d_rx, d_rz, d_img_pp, d_img_ps, false);
+    return rtm_batch_impl(ctx, 1, shot, d_wavelet, d_rx ? &d_rx : nullptr, d_rz ? &d_rz : nullptr, &d_img_pp,
+                          &d_img_ps, false);
+}
+
+int ouc_rtm_batch(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const float* wavelet, const float* const* rx,
+                  const float* const* rz, float* const* ipp, float* const* ips) {
+    return rtm_batch_impl(ctx, nshots, shots, wavelet, rx, rz, ipp, ips, true);
+}
+
+int ouc_rtm_batch_dev(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const float* d_wavelet, const float* const* rx,
+                      const float* const* rz, float* const* ipp, float* const* ips) {
+    return rtm_batch_impl(ctx, nshots, shots, d_wavelet, rx, rz, ipp, ips, false);
 }
 
 int ouc_stack(ouc_ctx* ctx, double* pp, double* ps, double* illum, int reset) {
@@ -672,7 +721,6 @@ int ouc_stack(ouc_ctx* ctx, double* pp, double* ps, double* illum, int reset) {
     if (reset)
         for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->d_stack[k], 0, ni * 8, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (reset) ctx->stacked = false;
     return OUC_OK;
 }
 

@@ -1,29 +1,44 @@
 // Fused time-step kernel of the elastic P/S-decoupled staggered-grid
 // scheme (sm_100a).
 //
-// One launch advances one wavefield by one time step.  The reference does it
-// in two launches that talk through six full-grid HBM arrays (forward_s then
-// forward_u, PS:2261-2264; rt_s_res/rt_u_res; reshot_u/reshot_s).  Here each
-// CTA owns a TX x TZ tile of cells and, in three phases separated by
-// __syncthreads():
-//   1. loads the total displacement U = P + S of its tile plus a 2N halo
-//      into shared memory (float4 loads along the contiguous z axis);
+// One launch advances one wavefield per shot of a batch by one time step.
+// The reference does it in two launches that talk through six full-grid
+// HBM arrays (forward_s then forward_u, PS:2261-2264; rt_s_res/rt_u_res;
+// reshot_u/reshot_s).  Here each CTA owns a TX x TZ tile of one shot
+// (blockIdx.y = shot) and, in three phases separated by __syncthreads():
+//   1. loads the total displacement U = P + S of its tile plus a 2N halo into
+//      shared memory (float4 loads along the contiguous z axis);
 //   2. computes the S-stage (theta, omega and the four Q fields, with the
-//      S-stage CPML memory) for its tile plus an N halo, keeping it on chip
-//      -- the halo cells are recomputed by both neighbouring CTAs, so the six
+//      S-stage CPML memory) for its tile plus an N halo, keeping it on chip:
+//      halo cells are recomputed by both neighbouring CTAs, so the six
 //      intermediate fields never reach HBM;
 //   3. computes the U-stage for its own cells: eight staggered derivatives of
-//      the S fields, U-stage CPML memory, the P/S leapfrog, and writes the
-//      new level over the oldest one (ping-pong of the P/S pairs makes the
-//      halo reads of phase 1 race-free).
+//      the S fields, the U-stage CPML memory, the P/S leapfrog, and writes the
+//      new level over the oldest one (ping-pong of the P/S pairs makes the halo
+//      reads of phase 1 race-free).
 // Receiver extraction, record injection, boundary-strip save/restore and the
 // zero-lag imaging condition ride along in the same launch.
 //
-// Arithmetic follows the reference operation by operation (coefficient sums
-// in k order then divided by the spacing, PS:229; the CPML update form of
-// PS:281; the leapfrog bracket order of PS:291-294), and memory terms that
-// are identically zero outside the damping layers are skipped, which leaves
-// every rounding unchanged.
+// Cost structure.  Tiles whose whole neighbourhood lies inside the update
+// domain, away from the boundary ring, the source and the receiver row are
+// "clean" and run no per-cell test at all; the few "edge" tiles mask per
+// float4.  Damping and edge handling are uniform run-time branches of a
+// single code path: separate unrolled variants per tile class overflow the
+// instruction cache.  Arithmetic is written with explicit roundings that reproduce the
+// reference's compiled expressions exactly (established by probing the
+// compiler's contractions on sm_100a):
+//   derivative  acc = fma(a_1, d_1, a_2 d_2);  acc = fma(a_k, d_k, acc);  acc / h
+//   CPML        fma(fma(d, e, -(d m)), dt, m)              (PS:281, PS:368)
+//   leapfrog    fma(dt^2, s, fma(2, now, -past))           (PS:291-294)
+//   imaging     acc + fma(p, q, u v)                       (PS:1434-1436)
+// which lets x-derivatives and all per-cell updates run as packed f32x2
+// instructions (two lanes of one float4 per instruction) without changing a
+// single rounding.  Division by the spacing uses the Markstein correction
+//   q0 = x r;  q = fma(fma(-q0, h, x), r, q0),   r = RN(1/h),
+// which returns the correctly rounded quotient for every normal result
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990; checked exhaustively against
+// IEEE division on sm_100a for the spacings in use); accumulators below
+// 2^-112 in magnitude take the IEEE division instead.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -60,48 +75,97 @@ struct TileGeo {
     static_assert((TX / 2) * (TZ / 4) == kThreads, "one U item per thread");
 };
 
+// ---- small helpers -----------------------------------------------------------
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float4 cat4(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float comp(const float4& v, int k) {
     return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
 }
 __device__ __forceinline__ void set_comp(float4& v, int k, float x) {
     if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
 }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b with one rounding: fma(b, -1, a)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return cat4(add2(lo2(a), lo2(b)), add2(hi2(a), hi2(b))); }
+__device__ __forceinline__ float4 sub4(float4 a, float4 b) { return cat4(sub2(lo2(a), lo2(b)), sub2(hi2(a), hi2(b))); }
+__device__ __forceinline__ float4 mul4(float4 a, float4 b) { return cat4(mul2(lo2(a), lo2(b)), mul2(hi2(a), hi2(b))); }
+__device__ __forceinline__ float4 mul4s(float4 a, float s) { return cat4(mul2(lo2(a), dup2(s)), mul2(hi2(a), dup2(s))); }
+__device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
-// CPML memory update m + (d*e - d*m)*dt, the form of PS:281 and PS:368.
-__device__ __forceinline__ float cpml1(float m, float d, float e, float dt) { return m + (d * e - d * m) * dt; }
+struct Div {
+    float h, r;   // spacing and RN(1/h)
+};
+constexpr float kTinyAcc = 0x1p-112f;
+
+__device__ __forceinline__ bool tiny(float x) { return fabsf(x) < kTinyAcc && x != 0.f; }
+__device__ __forceinline__ float mark1(float x, const Div& d) {
+    const float q0 = __fmul_rn(x, d.r);
+    return __fmaf_rn(__fmaf_rn(-q0, d.h, x), d.r, q0);
+}
+__device__ __forceinline__ float2 mark2(float2 x, const Div& d) {
+    const float2 q0 = mul2(x, dup2(d.r));
+    return fma2(fma2(q0, dup2(-d.h), x), dup2(d.r), q0);
+}
+// Four quotients; accumulators near the subnormal range (rare, at the
+// leading edge of a wavefront) take IEEE division instead.
+__device__ __forceinline__ float4 div4(float4 x, const Div& d) {
+    float4 q = cat4(mark2(lo2(x), d), mark2(hi2(x), d));
+    if (tiny(x.x) || tiny(x.y) || tiny(x.z) || tiny(x.w))
+        q = make_float4(__fdiv_rn(x.x, d.h), __fdiv_rn(x.y, d.h), __fdiv_rn(x.z, d.h), __fdiv_rn(x.w, d.h));
+    return q;
+}
+// CPML memory update fma(fma(d, e, -(d m)), dt, m), packed
+__device__ __forceinline__ float2 cpml2(float2 m, float2 d, float2 e, float dt) {
+    const float2 dm = mul2(d, m);
+    return fma2(fma2(d, e, make_float2(-dm.x, -dm.y)), dup2(dt), m);
+}
+__device__ __forceinline__ float4 cpml4(float4 m, float4 d, float4 e, float dt) {
+    return cat4(cpml2(lo2(m), lo2(d), lo2(e), dt), cpml2(hi2(m), hi2(d), hi2(e), dt));
+}
 
 // Staggered derivative of four consecutive z cells starting at `row`
 // (16-byte aligned shared-memory pointer at the first of the four cells).
 // PLUS: sum_k a_k (f[j+k] - f[j-k+1]);  MINUS: sum_k a_k (f[j+k-1] - f[j-k]).
+// Scalar: the z-shifted pairs do not sit in aligned register pairs.
 template <int N, bool PLUS>
-__device__ __forceinline__ float4 dz4(const float* row, const float* a, float h) {
+__device__ __forceinline__ float4 dz4(const float* row, const float* a, const Div& dv) {
     constexpr int NB = (N + 3) / 4;
     float w[4 * (2 * NB + 1)];
 #pragma unroll
     for (int b = 0; b < 2 * NB + 1; ++b) {
-        float4 v = ld4(row + 4 * (b - NB));
+        const float4 v = ld4(row + 4 * (b - NB));
         w[4 * b + 0] = v.x; w[4 * b + 1] = v.y; w[4 * b + 2] = v.z; w[4 * b + 3] = v.w;
     }
     float o[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int c = 4 * NB + q;
-        float acc = PLUS ? a[0] * (w[c + 1] - w[c]) : a[0] * (w[c] - w[c - 1]);
+        // fma(a_1, d_1, a_2 d_2), then fma(a_k, d_k, acc)
+        const float d0 = PLUS ? __fsub_rn(w[c + 1], w[c]) : __fsub_rn(w[c], w[c - 1]);
+        const float d1 = PLUS ? __fsub_rn(w[c + 2], w[c - 1]) : __fsub_rn(w[c + 1], w[c - 2]);
+        float acc = __fmaf_rn(a[0], d0, __fmul_rn(a[1], d1));
 #pragma unroll
-        for (int k = 1; k < N; ++k)
-            acc = PLUS ? acc + a[k] * (w[c + k + 1] - w[c - k]) : acc + a[k] * (w[c + k] - w[c - k - 1]);
-        o[q] = acc / h;
+        for (int k = 2; k < N; ++k)
+            acc = PLUS ? __fmaf_rn(a[k], __fsub_rn(w[c + k + 1], w[c - k]), acc)
+                       : __fmaf_rn(a[k], __fsub_rn(w[c + k], w[c - k - 1]), acc);
+        o[q] = acc;
     }
-    return make_float4(o[0], o[1], o[2], o[3]);
+    return div4(make_float4(o[0], o[1], o[2], o[3]), dv);
 }
 
-// Staggered x derivatives of RR consecutive rows of one float4 column.
-// `col` points at row r0 of the column in shared memory, `st` is the row
-// stride in floats.  Window rows r0-N .. r0+RR-1+N are read once.
+// Staggered x derivatives of RR consecutive rows of one float4 column,
+// packed two lanes per instruction.  `col` points at row r0 of the column in
+// shared memory, `st` is the row stride in floats; window rows r0-N ..
+// r0+RR-1+N are read once.
 template <int N, int RR, bool PLUS>
-__device__ __forceinline__ void dx4(const float* col, int st, const float* a, float h, float4 (&out)[RR]) {
+__device__ __forceinline__ void dx4(const float* col, int st, const float* a, const Div& dv, float4 (&out)[RR]) {
     float4 w[RR + 2 * N];
 #pragma unroll
     for (int k = 0; k < RR + 2 * N; ++k) {
@@ -110,32 +174,72 @@ __device__ __forceinline__ void dx4(const float* col, int st, const float* a, fl
 #pragma unroll
     for (int q = 0; q < RR; ++q) {
         const int c = q + N;
-        float4 acc;
-        if (PLUS) {
-            acc.x = a[0] * (w[c + 1].x - w[c].x); acc.y = a[0] * (w[c + 1].y - w[c].y);
-            acc.z = a[0] * (w[c + 1].z - w[c].z); acc.w = a[0] * (w[c + 1].w - w[c].w);
-        } else {
-            acc.x = a[0] * (w[c].x - w[c - 1].x); acc.y = a[0] * (w[c].y - w[c - 1].y);
-            acc.z = a[0] * (w[c].z - w[c - 1].z); acc.w = a[0] * (w[c].w - w[c - 1].w);
+        float2 acl, ach;
+        {   // fma(a_1, d_1, a_2 d_2)
+            const int hi0 = PLUS ? c + 1 : c, lo0 = PLUS ? c : c - 1;
+            const int hi1 = PLUS ? c + 2 : c + 1, lo1 = PLUS ? c - 1 : c - 2;
+            acl = fma2(dup2(a[0]), sub2(lo2(w[hi0]), lo2(w[lo0])), mul2(dup2(a[1]), sub2(lo2(w[hi1]), lo2(w[lo1]))));
+            ach = fma2(dup2(a[0]), sub2(hi2(w[hi0]), hi2(w[lo0])), mul2(dup2(a[1]), sub2(hi2(w[hi1]), hi2(w[lo1]))));
         }
 #pragma unroll
-        for (int k = 1; k < N; ++k) {
+        for (int k = 2; k < N; ++k) {
             const int hi = PLUS ? c + k + 1 : c + k, lo = PLUS ? c - k : c - k - 1;
-            acc.x = acc.x + a[k] * (w[hi].x - w[lo].x);
-            acc.y = acc.y + a[k] * (w[hi].y - w[lo].y);
-            acc.z = acc.z + a[k] * (w[hi].z - w[lo].z);
-            acc.w = acc.w + a[k] * (w[hi].w - w[lo].w);
+            acl = fma2(dup2(a[k]), sub2(lo2(w[hi]), lo2(w[lo])), acl);
+            ach = fma2(dup2(a[k]), sub2(hi2(w[hi]), hi2(w[lo])), ach);
         }
-        out[q] = make_float4(acc.x / h, acc.y / h, acc.z / h, acc.w / h);
+        out[q] = div4(cat4(acl, ach), dv);
     }
 }
 
-template <int N, int MODE, bool PX, bool PZ>
-__device__ __forceinline__ void step_tile(const StepArgs& p, float* sm, int x0, int z0) {
+// Per-launch, per-shot constants.
+struct ShotView {
+    int sx, sz, rz, src_type;
+    const float* wavelet;
+    float* rec_x;          // gather row t (kFwd) or nullptr
+    float* rec_z;
+    const float* inj_x;    // gather row t (kRcv)
+    const float* inj_z;
+    float* strip_save;     // kFwd: slot t
+    const float* strip_u;  // kRec: U slot
+    const float* strip_s;  // kRec: theta..Qxz slot
+    size_t off;            // state offset of this shot (floats)
+};
+
+__device__ __forceinline__ ShotView shot_view(const StepArgs& p, int b) {
+    const ShotDesc& d = p.shots[b];
+    ShotView v;
+    v.sx = d.sx; v.sz = d.sz; v.rz = d.rz; v.src_type = d.src_type;
+    v.wavelet = d.wavelet;
+    v.rec_x = p.record ? d.gather_x + (size_t)p.t * p.X : nullptr;
+    v.rec_z = p.record ? d.gather_z + (size_t)p.t * p.X : nullptr;
+    v.inj_x = d.gather_x + (size_t)p.t * p.X;
+    v.inj_z = d.gather_z + (size_t)p.t * p.X;
+    v.strip_save = (p.save && d.strips) ? d.strips + (size_t)p.t * p.strip_slot : nullptr;
+    v.strip_u = d.strips ? d.strips + (size_t)p.slot_u * p.strip_slot : nullptr;
+    v.strip_s = d.strips ? d.strips + (size_t)p.slot_s * p.strip_slot : nullptr;
+    v.off = (size_t)b * p.shot_stride;
+    return v;
+}
+
+// Per-component masks in edge tiles.
+template <int N, int MODE>
+__device__ __forceinline__ bool s_live(const StepArgs& p, int gi, int gj) {
+    if (MODE == kRec) return p.ring.in_box(gi, gj);
+    return gi >= N && gi < p.X - N && gj >= N && gj < p.Z - N;
+}
+template <int N, int MODE>
+__device__ __forceinline__ bool u_live(const StepArgs& p, int gi, int gj) {
+    if (MODE == kRec) return gi >= p.L && gi < p.X - p.L && gj >= p.L && gj < p.Z - p.L;
+    return gi >= N && gi < p.X - N && gj >= N && gj < p.Z - N;
+}
+
+template <int N, int MODE>
+__device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv, float* sm, int x0, int z0,
+                                          const bool PX, const bool PZ, const bool EDGE) {
     using G = TileGeo<N>;
     constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS, HU = G::HU, UC = G::UC, SC = G::SC;
     const int tid = threadIdx.x;
-    const int X = p.X, Z = p.Z, P = p.pitch, L = p.L;
+    const int P = p.pitch;
     float* sUx = sm + G::oUx;
     float* sUz = sm + G::oUz;
     float* sTh = sm + G::oTh;
@@ -147,41 +251,42 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, float* sm, int x0, 
     float a[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) a[k] = p.a[k];
+    const Div dvx{p.dx, p.rdx}, dvz{p.dz, p.rdz};
+    const size_t off = sv.off;
+    const float* nowp[4] = {p.now[0] + off, p.now[1] + off, p.now[2] + off, p.now[3] + off};
 
     // ---- phase 1: U = P + S over the tile and a 2N halo ---------------------
     for (int idx = tid; idx < G::UR * (UC / 4); idx += kThreads) {
         const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
         const int gi = x0 - SHX - N + r, gj = z0 - HU + 4 * c4;
         const ptrdiff_t g = (ptrdiff_t)gi * P + gj;
-        const float4 px = ld4(p.now[0] + g), pz = ld4(p.now[1] + g);
-        const float4 qx = ld4(p.now[2] + g), qz = ld4(p.now[3] + g);
-        float4 ux = make_float4(px.x + qx.x, px.y + qx.y, px.z + qx.z, px.w + qx.w);
-        float4 uz = make_float4(pz.x + qz.x, pz.y + qz.y, pz.z + qz.z, pz.w + qz.w);
-        if (MODE == kRcv) {
-            // load_record (PS:1471-1483): the receiver row is overwritten by the
-            // record over the interior x range before the S-stage reads it
-            if (p.inj_x && gi >= L && gi < X - L && p.rz >= gj && p.rz < gj + 4) {
-                set_comp(ux, p.rz - gj, p.inj_x[gi]);
-                set_comp(uz, p.rz - gj, p.inj_z[gi]);
+        float4 ux = add4(ld4(nowp[0] + g), ld4(nowp[2] + g));   // Ux = Px + Sx (PS:302)
+        float4 uz = add4(ld4(nowp[1] + g), ld4(nowp[3] + g));
+        if (EDGE) {
+            if (MODE == kRcv) {
+                // load_record (PS:1471-1483): the receiver row is overwritten by
+                // the record over the interior x range before the S-stage reads it
+                if (gi >= p.L && gi < p.X - p.L && sv.rz >= gj && sv.rz < gj + 4) {
+                    set_comp(ux, sv.rz - gj, sv.inj_x[gi]);
+                    set_comp(uz, sv.rz - gj, sv.inj_z[gi]);
+                }
             }
-        }
-        if (MODE == kRec) {
-            // reconstruction: the ring comes from the saved strips, cells
-            // outside the box are never read by the interior update
+            if (MODE == kRec) {
+                // reconstruction: ring cells come from the saved strips; cells
+                // outside the box are never read by the interior update
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int j = gj + k;
-                float vx = comp(ux, k), vz = comp(uz, k);
-                if (!p.ring.in_box(gi, j)) {
-                    vx = 0.f; vz = 0.f;
-                } else {
-                    const int ri = p.ring.index(gi, j);
-                    if (ri >= 0) {
-                        vx = p.strip_u[(size_t)kSUx * p.ring.R + ri];
-                        vz = p.strip_u[(size_t)kSUz * p.ring.R + ri];
+                for (int k = 0; k < 4; ++k) {
+                    const int j = gj + k;
+                    if (!p.ring.in_box(gi, j)) {
+                        set_comp(ux, k, 0.f); set_comp(uz, k, 0.f);
+                    } else {
+                        const int ri = p.ring.index(gi, j);
+                        if (ri >= 0) {
+                            set_comp(ux, k, sv.strip_u[(size_t)kSUx * p.ring.R + ri]);
+                            set_comp(uz, k, sv.strip_u[(size_t)kSUz * p.ring.R + ri]);
+                        }
                     }
                 }
-                set_comp(ux, k, vx); set_comp(uz, k, vz);
             }
         }
         st4(sUx + r * UC + 4 * c4, ux);
@@ -192,7 +297,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, float* sm, int x0, 
     // ---- phase 2: S-stage on the tile plus an N halo -------------------------
     if (tid < G::itemsA + G::itemsB) {
         int r0, c;
-        bool groupA = tid < G::itemsA;
+        const bool groupA = tid < G::itemsA;
         if (groupA) {
             r0 = -SHX + 4 * (tid / (TZ / 4));
             c = 4 * (tid % (TZ / 4));
@@ -202,93 +307,86 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, float* sm, int x0, 
             const int cc = k % (2 * HS / 4);
             c = cc < HS / 4 ? -HS + 4 * cc : TZ + 4 * (cc - HS / 4);
         }
-        // U shared-memory coordinates of (r0, c)
         const float* ux0 = sUx + (r0 + SHX + N) * UC + (c + HU);
         const float* uz0 = sUz + (r0 + SHX + N) * UC + (c + HU);
         float4 exx[4], ezx[4];
-        dx4<N, 4, false>(ux0, UC, a, p.dx, exx);   // dvxdx = D-x Ux
-        dx4<N, 4, true>(uz0, UC, a, p.dx, ezx);    // dvzdx = D+x Uz
+        dx4<N, 4, false>(ux0, UC, a, dvx, exx);   // dvxdx = D-x Ux
+        dx4<N, 4, true>(uz0, UC, a, dvx, ezx);    // dvzdx = D+x Uz
+        const bool ownc = c >= 0 && c < TZ;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = r0 + q;
             const int gi = x0 + r;
             const int gjb = z0 + c;
-            const float4 exz = dz4<N, true>(ux0 + q * UC, a, p.dz);    // dvxdz = D+z Ux
-            const float4 ezz = dz4<N, false>(uz0 + q * UC, a, p.dz);   // dvzdz = D-z Uz
+            const float4 exz = dz4<N, true>(ux0 + q * UC, a, dvz);    // dvxdz = D+z Ux
+            const float4 ezz = dz4<N, false>(uz0 + q * UC, a, dvz);   // dvzdz = D-z Uz
             const ptrdiff_t g = (ptrdiff_t)gi * P + gjb;
             const float4 vp2 = ld4(p.vp2 + g), vs2 = ld4(p.vs2 + g);
-            const bool own = r >= 0 && r < TX && c >= 0 && c < TZ;
-            float4 fo[4], fn[4];
-            float4 axv = make_float4(0.f, 0.f, 0.f, 0.f), azv = axv;
-            if (PX) { axv = ld4(p.ax + g); fo[0] = ld4(p.f_old[0] + g); fo[3] = ld4(p.f_old[3] + g); }
-            if (PZ) { azv = ld4(p.az + g); fo[1] = ld4(p.f_old[1] + g); fo[2] = ld4(p.f_old[2] + g); }
-            float4 th, om, qzx, qzz, qxx, qxz;
+            const bool own = ownc && r >= 0 && r < TX;
+            float4 fxx = zero4(), fzz = zero4(), fxz = zero4(), fzx = zero4();
+            if (PX) {
+                const float4 axv = ld4(p.ax + g);
+                fxx = cpml4(ld4(p.f_old[0] + off + g), axv, exx[q], p.dt);
+                fzx = cpml4(ld4(p.f_old[3] + off + g), axv, ezx[q], p.dt);
+            }
+            if (PZ) {
+                const float4 azv = ld4(p.az + g);
+                fzz = cpml4(ld4(p.f_old[1] + off + g), azv, ezz, p.dt);
+                fxz = cpml4(ld4(p.f_old[2] + off + g), azv, exz, p.dt);
+            }
+            // theta = Vp^2 (exx + ezz - Fxx - Fzz), omega = Vs^2 (exz - ezx - Fxz + Fzx) (PS:373-378);
+            // outside the damping layers the memories are exact zeros and
+            // adding or subtracting them leaves every rounding unchanged
+            float4 th = mul4(vp2, sub4(sub4(add4(exx[q], ezz), fxx), fzz));
+            float4 om = mul4(vs2, add4(sub4(sub4(exz, ezx[q]), fxz), fzx));
+            float4 qzx = mul4(vs2, sub4(ezx[q], fzx));
+            float4 qzz = mul4(vs2, sub4(ezz, fzz));
+            float4 qxz = mul4(vs2, sub4(exz, fxz));
+            float4 qxx = mul4(vs2, sub4(exx[q], fxx));
+            if (EDGE) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int gj = gjb + k;
-                const float e_xx = comp(exx[q], k), e_zx = comp(ezx[q], k);
-                const float e_xz = comp(exz, k), e_zz = comp(ezz, k);
-                const float vp2k = comp(vp2, k), vs2k = comp(vs2, k);
-                float fxx = 0.f, fzz = 0.f, fxz = 0.f, fzx = 0.f;
-                if (PX) {
-                    fxx = cpml1(comp(fo[0], k), comp(axv, k), e_xx, p.dt);
-                    fzx = cpml1(comp(fo[3], k), comp(axv, k), e_zx, p.dt);
-                }
-                if (PZ) {
-                    fzz = cpml1(comp(fo[1], k), comp(azv, k), e_zz, p.dt);
-                    fxz = cpml1(comp(fo[2], k), comp(azv, k), e_xz, p.dt);
-                }
-                float sth = e_xx + e_zz;
-                if (PX) sth = sth - fxx;
-                if (PZ) sth = sth - fzz;
-                float som = e_xz - e_zx;
-                if (PZ) som = som - fxz;
-                if (PX) som = som + fzx;
-                float v_th = vp2k * sth;
-                float v_om = vs2k * som;
-                float v_qzx = vs2k * (PX ? e_zx - fzx : e_zx);
-                float v_qzz = vs2k * (PZ ? e_zz - fzz : e_zz);
-                float v_qxz = vs2k * (PZ ? e_xz - fxz : e_xz);
-                float v_qxx = vs2k * (PX ? e_xx - fxx : e_xx);
-                bool live;
-                if (MODE == kRec) {
-                    live = p.ring.in_box(gi, gj);
-                    if (live && p.src_recon && gi == p.sx && gj == p.sz) v_th = v_th + p.wavelet[p.src_t];
-                    const int ri = live ? p.ring.index(gi, gj) : -1;
-                    if (ri >= 0) {
-                        const float* s = p.strip_s;
-                        const size_t R = p.ring.R;
-                        v_th = s[kSTh * R + ri]; v_om = s[kSOm * R + ri];
-                        v_qzx = s[kSQzx * R + ri]; v_qzz = s[kSQzz * R + ri];
-                        v_qxx = s[kSQxx * R + ri]; v_qxz = s[kSQxz * R + ri];
+                for (int k = 0; k < 4; ++k) {
+                    const int gj = gjb + k;
+                    float v_th = comp(th, k);
+                    bool live = s_live<N, MODE>(p, gi, gj);
+                    // source term on theta after the Q fields (PS:380)
+                    if (MODE == kFwd && sv.src_type == 0 && gi == sv.sx && gj == sv.sz) v_th = v_th + sv.wavelet[p.t];
+                    if (MODE == kRec) {
+                        if (live && p.src_recon && gi == sv.sx && gj == sv.sz) v_th = v_th + sv.wavelet[p.t + 1];
+                        const int ri = live ? p.ring.index(gi, gj) : -1;
+                        if (ri >= 0) {
+                            const float* s = sv.strip_s;
+                            const size_t R = p.ring.R;
+                            v_th = s[kSTh * R + ri];
+                            set_comp(om, k, s[kSOm * R + ri]);
+                            set_comp(qzx, k, s[kSQzx * R + ri]);
+                            set_comp(qzz, k, s[kSQzz * R + ri]);
+                            set_comp(qxx, k, s[kSQxx * R + ri]);
+                            set_comp(qxz, k, s[kSQxz * R + ri]);
+                        }
                     }
-                } else {
-                    live = gi >= N && gi < X - N && gj >= N && gj < Z - N;
-                    if (MODE == kFwd && p.src_type == 0 && gi == p.sx && gj == p.sz) v_th = v_th + p.wavelet[p.src_t];
-                }
-                if (!live) {
-                    v_th = v_om = v_qzx = v_qzz = v_qxz = v_qxx = 0.f;
-                    fxx = fzz = fxz = fzx = 0.f;
-                }
-                set_comp(th, k, v_th); set_comp(om, k, v_om);
-                set_comp(qzx, k, v_qzx); set_comp(qzz, k, v_qzz);
-                set_comp(qxx, k, v_qxx); set_comp(qxz, k, v_qxz);
-                if (PX) { set_comp(fn[0], k, fxx); set_comp(fn[3], k, fzx); }
-                if (PZ) { set_comp(fn[1], k, fzz); set_comp(fn[2], k, fxz); }
-                if (MODE == kFwd && own && p.strip_save) {
-                    const int ri = p.ring.index(gi, gj);
-                    if (ri >= 0) {
-                        float* s = p.strip_save;
-                        const size_t R = p.ring.R;
-                        s[kSTh * R + ri] = v_th; s[kSOm * R + ri] = v_om;
-                        s[kSQzx * R + ri] = v_qzx; s[kSQzz * R + ri] = v_qzz;
-                        s[kSQxx * R + ri] = v_qxx; s[kSQxz * R + ri] = v_qxz;
+                    if (!live) {
+                        v_th = 0.f;
+                        set_comp(om, k, 0.f); set_comp(qzx, k, 0.f); set_comp(qzz, k, 0.f);
+                        set_comp(qxx, k, 0.f); set_comp(qxz, k, 0.f);
+                        set_comp(fxx, k, 0.f); set_comp(fzz, k, 0.f); set_comp(fxz, k, 0.f); set_comp(fzx, k, 0.f);
+                    }
+                    set_comp(th, k, v_th);
+                    if (MODE == kFwd && own && sv.strip_save) {
+                        const int ri = p.ring.index(gi, gj);
+                        if (ri >= 0) {
+                            float* s = sv.strip_save;
+                            const size_t R = p.ring.R;
+                            s[kSTh * R + ri] = v_th; s[kSOm * R + ri] = comp(om, k);
+                            s[kSQzx * R + ri] = comp(qzx, k); s[kSQzz * R + ri] = comp(qzz, k);
+                            s[kSQxx * R + ri] = comp(qxx, k); s[kSQxz * R + ri] = comp(qxz, k);
+                        }
                     }
                 }
             }
             if (own) {
-                if (PX) { st4(p.f_new[0] + g, fn[0]); st4(p.f_new[3] + g, fn[3]); }
-                if (PZ) { st4(p.f_new[1] + g, fn[1]); st4(p.f_new[2] + g, fn[2]); }
+                if (PX) { st4(p.f_new[0] + off + g, fxx); st4(p.f_new[3] + off + g, fzx); }
+                if (PZ) { st4(p.f_new[1] + off + g, fzz); st4(p.f_new[2] + off + g, fxz); }
             }
             const int sr = r + SHX, scol = c + HS;
             st4(sTh + sr * SC + scol, th);
@@ -311,125 +409,159 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, float* sm, int x0, 
         const int c = 4 * (tid % (TZ / 4));
         const int scol = c + HS;
         float4 tx[2], wx[2], dB[2], dE[2];
-        dx4<N, 2, true>(sTh + (rr + SHX) * SC + scol, SC, a, p.dx, tx);    // dthetadx = D+x theta
-        dx4<N, 2, false>(sOm + (rr + SHX) * SC + scol, SC, a, p.dx, wx);   // domegadx = D-x omega
-        dx4<N, 2, false>(sQxz + (rr + SHX) * TZ + c, TZ, a, p.dx, dB);     // dux_zdx = D-x Qxz
-        dx4<N, 2, true>(sQzz + (rr + SHX) * TZ + c, TZ, a, p.dx, dE);      // duz_zdx = D+x Qzz
+        dx4<N, 2, true>(sTh + (rr + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
+        dx4<N, 2, false>(sOm + (rr + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
+        dx4<N, 2, false>(sQxz + (rr + SHX) * TZ + c, TZ, a, dvx, dB);     // dux_zdx = D-x Qxz
+        dx4<N, 2, true>(sQzz + (rr + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
+        const float dt = p.dt;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int r = rr + q;
             const int gi = x0 + r;
             const ptrdiff_t g = (ptrdiff_t)gi * P + (z0 + c);
-            const float4 tz = dz4<N, true>(sTh + (r + SHX) * SC + scol, a, p.dz);    // dthetadz
-            const float4 wz = dz4<N, false>(sOm + (r + SHX) * SC + scol, a, p.dz);   // domegadz
-            const float4 dA = dz4<N, true>(sQxx + r * SC + scol, a, p.dz);           // dux_xdz = D+z Qxx
-            const float4 dC = dz4<N, false>(sQzx + r * SC + scol, a, p.dz);          // duz_xdz = D-z Qzx
-            float4 axv = make_float4(0.f, 0.f, 0.f, 0.f), azv = axv;
-            float4 om_[8];
-            if (PX) {
-                axv = ld4(p.ax + g);
-                om_[1] = ld4(p.o[1] + g); om_[2] = ld4(p.o[2] + g);
-                om_[4] = ld4(p.o[4] + g); om_[7] = ld4(p.o[7] + g);
-            }
+            const float4 tz = dz4<N, true>(sTh + (r + SHX) * SC + scol, a, dvz);    // dthetadz
+            const float4 wz = dz4<N, false>(sOm + (r + SHX) * SC + scol, a, dvz);   // domegadz
+            const float4 dA = dz4<N, true>(sQxx + r * SC + scol, a, dvz);           // dux_xdz = D+z Qxx
+            const float4 dC = dz4<N, false>(sQzx + r * SC + scol, a, dvz);          // duz_xdz = D-z Qzx
+            float4 oC = zero4(), oE = zero4(), oB = zero4(), oA = zero4();
+            float4 oTx = zero4(), oTz = zero4(), oWz = zero4(), oWx = zero4();
             if (PZ) {
-                azv = ld4(p.az + g);
-                om_[0] = ld4(p.o[0] + g); om_[3] = ld4(p.o[3] + g);
-                om_[5] = ld4(p.o[5] + g); om_[6] = ld4(p.o[6] + g);
+                const float4 d = ld4(p.az + g);
+                oC = cpml4(ld4(p.o[0] + off + g), d, dC, dt);
+                oA = cpml4(ld4(p.o[3] + off + g), d, dA, dt);
+                oTz = cpml4(ld4(p.o[5] + off + g), d, tz, dt);
+                oWz = cpml4(ld4(p.o[6] + off + g), d, wz, dt);
             }
-            const float4 npx = ld4(p.now[0] + g), npz = ld4(p.now[1] + g);
-            const float4 nsx = ld4(p.now[2] + g), nsz = ld4(p.now[3] + g);
-            const float4 opx = ld4(p.past[0] + g), opz = ld4(p.past[1] + g);
-            const float4 osx = ld4(p.past[2] + g), osz = ld4(p.past[3] + g);
-            float4 vpx, vpz, vsx, vsz, onew[8];
-            float4 rp[4], ac[3];
-            if (MODE == kRec) {
-                rp[0] = ld4(p.rcv[0] + g); rp[1] = ld4(p.rcv[1] + g); rp[2] = ld4(p.rcv[2] + g); rp[3] = ld4(p.rcv[3] + g);
-                ac[0] = ld4(p.acc[0] + g); ac[1] = ld4(p.acc[1] + g); ac[2] = ld4(p.acc[2] + g);
+            if (PX) {
+                const float4 d = ld4(p.ax + g);
+                oE = cpml4(ld4(p.o[1] + off + g), d, dE[q], dt);
+                oB = cpml4(ld4(p.o[2] + off + g), d, dB[q], dt);
+                oTx = cpml4(ld4(p.o[4] + off + g), d, tx[q], dt);
+                oWx = cpml4(ld4(p.o[7] + off + g), d, wx[q], dt);
             }
+            // leapfrog brackets in the reference's order (PS:291-294); zero
+            // memories outside the damping layers change no rounding
+            const float4 nwx = make_float4(-wx[q].x, -wx[q].y, -wx[q].z, -wx[q].w);
+            const float4 spx = add4(sub4(sub4(add4(sub4(tx[q], oTx), dC), dE[q]), oC), oE);
+            const float4 spz = add4(sub4(sub4(add4(sub4(tz, oTz), dB[q]), dA), oB), oA);
+            const float4 ssx = add4(sub4(sub4(add4(sub4(wz, oWz), dC), dE[q]), oC), oE);
+            const float4 ssz = add4(sub4(sub4(add4(add4(nwx, oWx), dB[q]), dA), oB), oA);
+            const float4 npx = ld4(nowp[0] + g), npz = ld4(nowp[1] + g);
+            const float4 nsx = ld4(nowp[2] + g), nsz = ld4(nowp[3] + g);
+            const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);
+            const float4 osx = ld4(p.past[2] + off + g), osz = ld4(p.past[3] + off + g);
+            const float2 two = dup2(2.f), dt2 = dup2(p.dt2), m1 = dup2(-1.f);
+            auto leap = [&](float4 now, float4 past, float4 s) {
+                return cat4(fma2(dt2, lo2(s), fma2(two, lo2(now), mul2(lo2(past), m1))),
+                            fma2(dt2, hi2(s), fma2(two, hi2(now), mul2(hi2(past), m1))));
+            };
+            float4 vpx = leap(npx, opx, spx), vpz = leap(npz, opz, spz);
+            float4 vsx = leap(nsx, osx, ssx), vsz = leap(nsz, osz, ssz);
+            if (EDGE) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int gj = z0 + c + k;
-                const float dtx = comp(tx[q], k), dtz = comp(tz, k), dwx = comp(wx[q], k), dwz = comp(wz, k);
-                const float A = comp(dA, k), B = comp(dB[q], k), Cc = comp(dC, k), E = comp(dE[q], k);
-                float oC = 0.f, oE = 0.f, oB = 0.f, oA = 0.f, oTx = 0.f, oTz = 0.f, oWz = 0.f, oWx = 0.f;
-                if (PZ) {
-                    const float d = comp(azv, k);
-                    oC = cpml1(comp(om_[0], k), d, Cc, p.dt);
-                    oA = cpml1(comp(om_[3], k), d, A, p.dt);
-                    oTz = cpml1(comp(om_[5], k), d, dtz, p.dt);
-                    oWz = cpml1(comp(om_[6], k), d, dwz, p.dt);
-                }
-                if (PX) {
-                    const float d = comp(axv, k);
-                    oE = cpml1(comp(om_[1], k), d, E, p.dt);
-                    oB = cpml1(comp(om_[2], k), d, B, p.dt);
-                    oTx = cpml1(comp(om_[4], k), d, dtx, p.dt);
-                    oWx = cpml1(comp(om_[7], k), d, dwx, p.dt);
-                }
-                // leapfrog brackets in the reference's order (PS:291-294)
-                float spx = dtx, spz = dtz, ssx = dwz, ssz = -dwx;
-                if (PX) spx = spx - oTx;
-                if (PZ) spz = spz - oTz;
-                if (PZ) ssx = ssx - oWz;
-                if (PX) ssz = ssz + oWx;
-                spx = spx + Cc - E; ssx = ssx + Cc - E;
-                spz = spz + B - A; ssz = ssz + B - A;
-                if (PZ) { spx = spx - oC; ssx = ssx - oC; }
-                if (PX) { spx = spx + oE; ssx = ssx + oE; }
-                if (PX) { spz = spz - oB; ssz = ssz - oB; }
-                if (PZ) { spz = spz + oA; ssz = ssz + oA; }
-                float v_px = 2 * comp(npx, k) - comp(opx, k) + p.dt2 * spx;
-                float v_pz = 2 * comp(npz, k) - comp(opz, k) + p.dt2 * spz;
-                float v_sx = 2 * comp(nsx, k) - comp(osx, k) + p.dt2 * ssx;
-                float v_sz = 2 * comp(nsz, k) - comp(osz, k) + p.dt2 * ssz;
-                bool live;
-                if (MODE == kRec) live = gi >= L && gi < X - L && gj >= L && gj < Z - L;
-                else live = gi >= N && gi < X - N && gj >= N && gj < Z - N;
-                if (MODE == kFwd && p.src_type == 1 && live && gi == p.sx && gj == p.sz)
-                    v_pz = v_pz + p.dt2 * p.wavelet[p.src_t];
-                if (!live) {
-                    v_px = v_pz = v_sx = v_sz = 0.f;
-                    oC = oE = oB = oA = oTx = oTz = oWz = oWx = 0.f;
-                }
-                set_comp(vpx, k, v_px); set_comp(vpz, k, v_pz);
-                set_comp(vsx, k, v_sx); set_comp(vsz, k, v_sz);
-                if (PZ) { set_comp(onew[0], k, oC); set_comp(onew[3], k, oA); set_comp(onew[5], k, oTz); set_comp(onew[6], k, oWz); }
-                if (PX) { set_comp(onew[1], k, oE); set_comp(onew[2], k, oB); set_comp(onew[4], k, oTx); set_comp(onew[7], k, oWx); }
-                if (MODE != kRcv) {
-                    const float v_ux = v_px + v_sx, v_uz = v_pz + v_sz;   // PS:302-303 / PS:978-979
-                    if (MODE == kFwd && p.rec_x && gj == p.rz && gi < X) {
-                        p.rec_x[gi] = v_ux;   // record the post-update value (PS:307-311)
-                        p.rec_z[gi] = v_uz;
+                for (int k = 0; k < 4; ++k) {
+                    const int gj = z0 + c + k;
+                    if (MODE == kFwd && sv.src_type == 1 && gi == sv.sx && gj == sv.sz)
+                        set_comp(vpz, k, comp(vpz, k) + p.dt2 * sv.wavelet[p.t]);
+                    if (!u_live<N, MODE>(p, gi, gj)) {
+                        set_comp(vpx, k, 0.f); set_comp(vpz, k, 0.f); set_comp(vsx, k, 0.f); set_comp(vsz, k, 0.f);
+                        set_comp(oC, k, 0.f); set_comp(oE, k, 0.f); set_comp(oB, k, 0.f); set_comp(oA, k, 0.f);
+                        set_comp(oTx, k, 0.f); set_comp(oTz, k, 0.f); set_comp(oWz, k, 0.f); set_comp(oWx, k, 0.f);
                     }
-                    if (MODE == kFwd && p.strip_save) {
-                        const int ri = p.ring.index(gi, gj);
+                }
+            }
+            if (MODE != kRcv) {
+                const float4 ux = add4(vpx, vsx), uz = add4(vpz, vsz);   // PS:302-303 / PS:978-979
+                if (MODE == kFwd && sv.rec_x && sv.rz >= z0 + c && sv.rz < z0 + c + 4 && gi < p.X) {
+                    sv.rec_x[gi] = comp(ux, sv.rz - z0 - c);   // post-update value (PS:307-311)
+                    sv.rec_z[gi] = comp(uz, sv.rz - z0 - c);
+                }
+                if (EDGE && MODE == kFwd && sv.strip_save) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int ri = p.ring.index(gi, z0 + c + k);
                         if (ri >= 0) {
-                            p.strip_save[(size_t)kSUx * p.ring.R + ri] = v_ux;
-                            p.strip_save[(size_t)kSUz * p.ring.R + ri] = v_uz;
+                            sv.strip_save[(size_t)kSUx * p.ring.R + ri] = comp(ux, k);
+                            sv.strip_save[(size_t)kSUz * p.ring.R + ri] = comp(uz, k);
                         }
                     }
                 }
-                if (MODE == kRec) {
-                    // zero-lag imaging condition (corr_v, PS:1426-1439) on the interior
-                    const float sx_ = p.img_past ? comp(opx, k) : comp(npx, k);
-                    const float sz_ = p.img_past ? comp(opz, k) : comp(npz, k);
-                    const float rpx = comp(rp[0], k), rpz = comp(rp[1], k), rsx = comp(rp[2], k), rsz = comp(rp[3], k);
-                    if (live) {
-                        set_comp(ac[0], k, comp(ac[0], k) + (sx_ * rpx + sz_ * rpz));
-                        set_comp(ac[2], k, comp(ac[2], k) + (sx_ * sx_ + sz_ * sz_));
-                        set_comp(ac[1], k, comp(ac[1], k) + (sx_ * rsx + sz_ * rsz));
-                    }
-                }
             }
             if (MODE == kRec) {
-                st4(p.acc[0] + g, ac[0]); st4(p.acc[1] + g, ac[1]); st4(p.acc[2] + g, ac[2]);
+                // zero-lag imaging condition (corr_v, PS:1426-1439) on the interior
+                const float4 sx = p.img_past ? opx : npx;
+                const float4 sz = p.img_past ? opz : npz;
+                const float4 rpx = ld4(p.rcv[0] + off + g), rpz = ld4(p.rcv[1] + off + g);
+                const float4 rsx = ld4(p.rcv[2] + off + g), rsz = ld4(p.rcv[3] + off + g);
+                float* acc0 = p.acc[0] + off + g;
+                float* acc1 = p.acc[1] + off + g;
+                float* acc2 = p.acc[2] + off + g;
+                auto corr = [&](float4 acc, float4 a1, float4 b1, float4 a2, float4 b2) {
+                    return cat4(add2(lo2(acc), fma2(lo2(a1), lo2(b1), mul2(lo2(a2), lo2(b2)))),
+                                add2(hi2(acc), fma2(hi2(a1), hi2(b1), mul2(hi2(a2), hi2(b2)))));
+                };
+                float4 npp = corr(ld4(acc0), sx, rpx, sz, rpz);
+                float4 nil = corr(ld4(acc2), sx, sx, sz, sz);
+                float4 nps = corr(ld4(acc1), sx, rsx, sz, rsz);
+                if (EDGE) {
+                    const float4 o0 = ld4(acc0), o1 = ld4(acc1), o2 = ld4(acc2);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (!u_live<N, MODE>(p, gi, z0 + c + k)) {
+                            set_comp(npp, k, comp(o0, k)); set_comp(nps, k, comp(o1, k)); set_comp(nil, k, comp(o2, k));
+                        }
+                    }
+                }
+                st4(acc0, npp); st4(acc1, nps); st4(acc2, nil);
             }
-            st4(p.past[0] + g, vpx); st4(p.past[1] + g, vpz);
-            st4(p.past[2] + g, vsx); st4(p.past[3] + g, vsz);
-            if (PZ) { st4(p.o[0] + g, onew[0]); st4(p.o[3] + g, onew[3]); st4(p.o[5] + g, onew[5]); st4(p.o[6] + g, onew[6]); }
-            if (PX) { st4(p.o[1] + g, onew[1]); st4(p.o[2] + g, onew[2]); st4(p.o[4] + g, onew[4]); st4(p.o[7] + g, onew[7]); }
+            st4(p.past[0] + off + g, vpx); st4(p.past[1] + off + g, vpz);
+            st4(p.past[2] + off + g, vsx); st4(p.past[3] + off + g, vsz);
+            if (PZ) {
+                st4(p.o[0] + off + g, oC); st4(p.o[3] + off + g, oA);
+                st4(p.o[5] + off + g, oTz); st4(p.o[6] + off + g, oWz);
+            }
+            if (PX) {
+                st4(p.o[1] + off + g, oE); st4(p.o[2] + off + g, oB);
+                st4(p.o[4] + off + g, oTx); st4(p.o[7] + off + g, oWx);
+            }
         }
     }
+}
+
+// Tile classification (uniform per CTA).
+template <int N, int MODE>
+__device__ __forceinline__ bool tile_is_edge(const StepArgs& p, const ShotView& sv, int x0, int z0) {
+    using G = TileGeo<N>;
+    const int X = p.X, Z = p.Z, L = p.L;
+    if (MODE == kRec) {
+        // clean: the whole U box lies in the deep interior (no ring, inside the box)
+        const int r0 = x0 - G::SHX - N, r1 = x0 + G::TX + G::SHX + N;
+        const int c0 = z0 - G::HU, c1 = z0 + G::TZ + G::HU;
+        bool clean = r0 >= L + N && r1 <= X - L - N && c0 >= L + N && c1 <= Z - L - N;
+        if (p.src_recon && sv.sx >= x0 - G::SHX && sv.sx < x0 + G::TX + G::SHX && sv.sz >= z0 - G::HS &&
+            sv.sz < z0 + G::TZ + G::HS)
+            clean = false;
+        return !clean;
+    }
+    bool clean = x0 - G::SHX >= N && x0 + G::TX + G::SHX <= X - N && z0 - G::HS >= N && z0 + G::TZ + G::HS <= Z - N;
+    if (MODE == kFwd) {
+        // source inside the S region
+        if (sv.sx >= x0 - G::SHX && sv.sx < x0 + G::TX + G::SHX && sv.sz >= z0 - G::HS && sv.sz < z0 + G::TZ + G::HS)
+            clean = false;
+        // own cells touching the boundary ring while saving strips
+        if (p.save) {
+            const int bx0 = L - N, bx1 = X - L + N, bz0 = L - N, bz1 = Z - L + N;       // box
+            const int dx0 = L + N, dx1 = X - L - N, dz0 = L + N, dz1 = Z - L - N;       // deep interior
+            const bool meets_box = x0 < bx1 && x0 + G::TX > bx0 && z0 < bz1 && z0 + G::TZ > bz0;
+            const bool inside_deep = x0 >= dx0 && x0 + G::TX <= dx1 && z0 >= dz0 && z0 + G::TZ <= dz1;
+            if (meets_box && !inside_deep) clean = false;
+        }
+    }
+    if (MODE == kRcv) {
+        // injection row inside the U box
+        if (sv.rz >= z0 - G::HU && sv.rz < z0 + G::TZ + G::HU) clean = false;
+    }
+    return !clean;
 }
 
 template <int N, int MODE>
@@ -439,18 +571,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
     using G = TileGeo<N>;
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
     const int x0 = (p.tile_x0 + tx) * G::TX, z0 = (p.tile_z0 + tz) * G::TZ;
+    const ShotView sv = shot_view(p, blockIdx.y);
+    const bool edge = tile_is_edge<N, MODE>(p, sv, x0, z0);
     if (MODE == kRec) {
-        step_tile<N, MODE, false, false>(p, sm, x0, z0);
+        step_tile<N, MODE>(p, sv, sm, x0, z0, false, false, edge);
         return;
     }
     // Damping is non-zero for i < L or i > X-L (PS:2072-2080); a tile takes
     // the memory-variable path when its S-stage halo touches such a cell.
     const bool px = (x0 - G::SHX < p.L) || (x0 + G::TX + G::SHX - 1 >= p.X - p.L);
     const bool pz = (z0 - G::HS < p.L) || (z0 + G::TZ + G::HS - 1 >= p.Z - p.L);
-    if (px && pz) step_tile<N, MODE, true, true>(p, sm, x0, z0);
-    else if (px) step_tile<N, MODE, true, false>(p, sm, x0, z0);
-    else if (pz) step_tile<N, MODE, false, true>(p, sm, x0, z0);
-    else step_tile<N, MODE, false, false>(p, sm, x0, z0);
+    step_tile<N, MODE>(p, sv, sm, x0, z0, px, pz, edge);
 }
 
 }  // namespace ouc

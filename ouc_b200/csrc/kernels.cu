@@ -9,32 +9,33 @@
 namespace ouc {
 
 template <int N, int MODE>
-static void launch_one(const StepArgs& a, int tiles_x, cudaStream_t s) {
+static void launch_one(const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
     constexpr int bytes = TileGeo<N>::bytes;
     static bool configured = false;   // one attribute call per instantiation
     if (!configured) {
         cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
         configured = true;
     }
-    k_step<N, MODE><<<tiles_x * a.tiles_z, kThreads, bytes, s>>>(a);
+    k_step<N, MODE><<<dim3(tiles_x * a.tiles_z, nshots), kThreads, bytes, s>>>(a);
 }
 
 template <int N>
-static int launch_mode(Mode m, const StepArgs& a, int tiles_x, cudaStream_t s) {
+static int launch_mode(Mode m, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
     switch (m) {
-        case kFwd: launch_one<N, kFwd>(a, tiles_x, s); return 0;
-        case kRcv: launch_one<N, kRcv>(a, tiles_x, s); return 0;
-        case kRec: launch_one<N, kRec>(a, tiles_x, s); return 0;
+        case kFwd: launch_one<N, kFwd>(a, tiles_x, nshots, s); return 0;
+        case kRcv: launch_one<N, kRcv>(a, tiles_x, nshots, s); return 0;
+        case kRec: launch_one<N, kRec>(a, tiles_x, nshots, s); return 0;
     }
     return 1;
 }
 
-int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, cudaStream_t s) {
+int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
     switch (N) {
-        case 2: return launch_mode<2>(mode, a, tiles_x, s);
-        case 4: return launch_mode<4>(mode, a, tiles_x, s);
-        case 5: return launch_mode<5>(mode, a, tiles_x, s);
-        case 6: return launch_mode<6>(mode, a, tiles_x, s);
+        case 2: return launch_mode<2>(mode, a, tiles_x, nshots, s);
+        case 5: return launch_mode<5>(mode, a, tiles_x, nshots, s);
+        case 6: return launch_mode<6>(mode, a, tiles_x, nshots, s);
     }
     return 1;
 }
@@ -42,7 +43,6 @@ int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, cudaStream_t s
 int step_smem_bytes(int N) {
     switch (N) {
         case 2: return TileGeo<2>::bytes;
-        case 4: return TileGeo<4>::bytes;
         case 5: return TileGeo<5>::bytes;
         case 6: return TileGeo<6>::bytes;
     }
@@ -55,8 +55,9 @@ int step_smem_bytes(int N) {
 // after the receiver's first back-step.
 __global__ void k_image_only(const StepArgs p) {
     const int i = blockIdx.y + p.L;
+    const size_t off = (size_t)blockIdx.z * p.shot_stride;
     for (int j = p.L + threadIdx.x + blockIdx.x * blockDim.x; j < p.Z - p.L; j += blockDim.x * gridDim.x) {
-        const ptrdiff_t g = (ptrdiff_t)i * p.pitch + j;
+        const ptrdiff_t g = (ptrdiff_t)i * p.pitch + j + off;
         const float sx = p.now[0][g], sz = p.now[1][g];
         p.acc[0][g] += sx * p.rcv[0][g] + sz * p.rcv[1][g];
         p.acc[2][g] += sx * sx + sz * sz;
@@ -64,9 +65,9 @@ __global__ void k_image_only(const StepArgs p) {
     }
 }
 
-void launch_image_only(const StepArgs& a, cudaStream_t s) {
+void launch_image_only(const StepArgs& a, int nshots, cudaStream_t s) {
     const int nx = a.X - 2 * a.L;
-    dim3 grid((a.Z - 2 * a.L + 255) / 256, nx);
+    dim3 grid((a.Z - 2 * a.L + 255) / 256, nx, nshots);
     k_image_only<<<grid, 256, 0, s>>>(a);
 }
 
@@ -82,29 +83,36 @@ __global__ void k_finalize(const FinalizeArgs f) {
     const int i = ii + f.L;
     for (int jj = threadIdx.x + blockIdx.x * blockDim.x; jj < nz; jj += blockDim.x * gridDim.x) {
         const int j = jj + f.L;
-        const ptrdiff_t g = (ptrdiff_t)i * f.pitch + j;
-        float lpp = 0.f, lps = 0.f;
-        if (i >= f.L + 2 && i < f.X - f.L - 2 && j >= f.L + 2 && j < f.Z - f.L - 2) {
-            const float* npp = f.acc[0];
-            const float* nps = f.acc[1];
-            const float* den = f.acc[2];
-            const ptrdiff_t P = f.pitch;
-            const float c = 1 / f.dh / f.dh;
-            lpp = c * (img_at(npp, den, g + P) + img_at(npp, den, g - P) - 2 * img_at(npp, den, g) +
-                       img_at(npp, den, g + 1) + img_at(npp, den, g - 1) - 2 * img_at(npp, den, g));
-            lps = c * (img_at(nps, den, g + P) + img_at(nps, den, g - P) - 2 * img_at(nps, den, g) +
-                       img_at(nps, den, g + 1) + img_at(nps, den, g - 1) - 2 * img_at(nps, den, g));
-        }
         const size_t o = (size_t)ii * nz + jj;
-        if (f.img_pp) f.img_pp[o] = lpp;
-        if (f.img_ps) f.img_ps[o] = lps;
+        double spp = 0.0, sps = 0.0, sil = 0.0;
+        for (int b = 0; b < f.nshots; ++b) {   // shots in order: the FP64 stack is deterministic
+            const ptrdiff_t g = (ptrdiff_t)i * f.pitch + j + (ptrdiff_t)(b * f.shot_stride);
+            float lpp = 0.f, lps = 0.f;
+            if (i >= f.L + 2 && i < f.X - f.L - 2 && j >= f.L + 2 && j < f.Z - f.L - 2) {
+                const float* npp = f.acc[0];
+                const float* nps = f.acc[1];
+                const float* den = f.acc[2];
+                const ptrdiff_t P = f.pitch;
+                const float c = 1 / f.dh / f.dh;
+                lpp = c * (img_at(npp, den, g + P) + img_at(npp, den, g - P) - 2 * img_at(npp, den, g) +
+                           img_at(npp, den, g + 1) + img_at(npp, den, g - 1) - 2 * img_at(npp, den, g));
+                lps = c * (img_at(nps, den, g + P) + img_at(nps, den, g - P) - 2 * img_at(nps, den, g) +
+                           img_at(nps, den, g + 1) + img_at(nps, den, g - 1) - 2 * img_at(nps, den, g));
+            }
+            if (f.img) {
+                f.img[((size_t)b * 2 + 0) * nx * nz + o] = lpp;
+                f.img[((size_t)b * 2 + 1) * nx * nz + o] = lps;
+            }
+            spp += (double)lpp;
+            sps += (double)lps;
+            sil += (double)f.acc[2][g];
+        }
         if (f.stack[0]) {
-            f.stack[0][o] += (double)lpp;
-            f.stack[1][o] += (double)lps;
-            f.stack[2][o] += (double)f.acc[2][g];
+            f.stack[0][o] += spp;
+            f.stack[1][o] += sps;
+            f.stack[2][o] += sil;
         }
     }
-    (void)nx;
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {

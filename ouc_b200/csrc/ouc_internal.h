@@ -61,59 +61,64 @@ struct Ring {
 // Ux, Uz, theta, omega, Qzx, Qzz, Qxx, Qxz.
 enum StripField : int { kSUx = 0, kSUz, kSTh, kSOm, kSQzx, kSQzz, kSQxx, kSQxz, kStripFields };
 
+// Per-shot constants of a batch (uploaded once per batch).
+struct ShotDesc {
+    int sx, sz, rz, src_type;      // padded coordinates
+    const float* wavelet;          // nt samples
+    float* gather_x;               // time-major gathers [nt][X]
+    float* gather_z;
+    float* strips;                 // [slot][8 fields][ring] or null
+};
+
 struct StepArgs {
     int X, Z, pitch, L;
     int tiles_z, tile_x0, tile_z0;    // tile grid of this launch
     int t;                            // time step index
+    int slot_u, slot_s;               // kRec: strip slots holding U and theta..Qxz at level t+1
+    int record, save;                 // kFwd: write gathers / boundary strips this step
+    int src_recon;                    // kRec: add the source term at (sx, sz) outside the ring
+    int img_past;                     // kRec: correlate with level t+2 (reference alignment)
     float a[6];                       // stencil weights a_1..a_N
     float dx, dz, dt, dt2;
+    float rdx, rdz;                   // RN(1/dx), RN(1/dz)
+    // Fields of shot 0; shot b adds b * shot_stride floats.
     // leapfrog state: now (level n, read with halo), past (level n-1, read
     // at own cells, overwritten with level n+1)
-    const float* __restrict__ now[4];   // Px Pz Sx Sz
-    float* __restrict__ past[4];
+    const float* now[4];              // Px Pz Sx Sz
+    float* past[4];
     // S-stage CPML memory, ping-pong: read old (halo), write new (own)
-    const float* __restrict__ f_old[4];  // xx zz xz zx
-    float* __restrict__ f_new[4];
+    const float* f_old[4];            // xx zz xz zx
+    float* f_new[4];
     // U-stage CPML memory, in place at own cells
-    float* __restrict__ o[8];            // C E B A Tx Tz Wz Wx
-    const float* __restrict__ vp2;
-    const float* __restrict__ vs2;
-    const float* __restrict__ ax;
-    const float* __restrict__ az;
-    // source: theta += wavelet[src_t] at (sx, sz) (kFwd, and kRec when src_recon)
-    int sx, sz, src_t, src_type, src_recon;
-    const float* __restrict__ wavelet;
-    // receivers: row rz; inj_* (kRcv) and rec_* (kFwd) point at row t of a
-    // time-major gather [nt][X]
-    int rz;
-    const float* __restrict__ inj_x;
-    const float* __restrict__ inj_z;
-    float* __restrict__ rec_x;
-    float* __restrict__ rec_z;
-    // boundary strips
-    Ring ring;
-    float* __restrict__ strip_save;         // kFwd: slot t (8 fields) or null
-    const float* __restrict__ strip_u;      // kRec: slot holding U at level t+1
-    const float* __restrict__ strip_s;      // kRec: slot holding theta..Qxz at level t+1
+    float* o[8];                      // C E B A Tx Tz Wz Wx
     // kRec imaging
-    const float* __restrict__ rcv[4];       // receiver Px Pz Sx Sz after this back-step
-    float* __restrict__ acc[3];             // PP, PS, illumination accumulators
-    int img_past;                           // 1: correlate with level t+2 (reference)
+    const float* rcv[4];              // receiver Px Pz Sx Sz after this back-step
+    float* acc[3];                    // PP, PS, illumination accumulators
+    // model (shared by the batch)
+    const float* vp2;
+    const float* vs2;
+    const float* ax;
+    const float* az;
+    size_t shot_stride;               // floats between consecutive shots' state
+    size_t strip_slot;                // floats per strip slot
+    Ring ring;
+    const ShotDesc* shots;            // device array indexed by blockIdx.y
 };
 
 struct FinalizeArgs {
     int X, Z, pitch, L;
+    int nshots;
+    size_t shot_stride;    // between shots' accumulators (floats)
     float dh;
-    const float* acc[3];
-    float* img_pp;     // nx*nz dense, or null
-    float* img_ps;
-    double* stack[3];  // nx*nz dense FP64: PP, PS, illumination (or null)
+    const float* acc[3];   // shot 0
+    float* img;            // [shot][2][nx][nz] dense, or null
+    double* stack[3];      // nx*nz dense FP64: PP, PS, illumination (or null)
 };
 
 // Host-side launchers (kernels.cu)
-int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, cudaStream_t s);
+int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s);
 int step_smem_bytes(int N);
-void launch_image_only(const StepArgs& a, cudaStream_t s);
+void launch_image_only(const StepArgs& a, int nshots, cudaStream_t s);
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s);
 void launch_mute(float* gx, float* gz, int X, int nt, int sx, int sz, int rz, int t0, float dt, float dh, float v,
                  cudaStream_t s);
