@@ -177,7 +177,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
                     help="c2: the headline 1000x500 RTM workload; c4: the 4000x1500 grid (HBM-bound profiling)")
     ap.add_argument("--ref-steps", type=int, default=None, help="CPU sample length (time steps)")
-    ap.add_argument("--batch", type=int, default=8, help="shots advanced together per step")
+    ap.add_argument("--batch", type=int, default=16, help="shots advanced together per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 

@@ -37,8 +37,8 @@
 //   q0 = x r;  q = fma(fma(-q0, h, x), r, q0),   r = RN(1/h),
 // which returns the correctly rounded quotient for every normal result
 // (P. Markstein, IBM J. Res. Dev. 34(1), 1990; checked exhaustively against
-// IEEE division on sm_100a for the spacings in use); accumulators below
-// 2^-112 in magnitude take the IEEE division instead.
+// IEEE division on sm_100a for the spacings in use); quotients near the
+// subnormal range go through double precision (div4 below).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -102,23 +102,22 @@ __device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.
 struct Div {
     float h, r;   // spacing and RN(1/h)
 };
-constexpr float kTinyAcc = 0x1p-112f;
 
-__device__ __forceinline__ bool tiny(float x) { return fabsf(x) < kTinyAcc && x != 0.f; }
-__device__ __forceinline__ float mark1(float x, const Div& d) {
-    const float q0 = __fmul_rn(x, d.r);
-    return __fmaf_rn(__fmaf_rn(-q0, d.h, x), d.r, q0);
-}
-__device__ __forceinline__ float2 mark2(float2 x, const Div& d) {
-    const float2 q0 = mul2(x, dup2(d.r));
-    return fma2(fma2(q0, dup2(-d.h), x), dup2(d.r), q0);
-}
-// Four quotients; accumulators near the subnormal range (rare, at the
-// leading edge of a wavefront) take IEEE division instead.
+// Quotients below 2^-124 (the subnormal neighbourhood, common ahead of a
+// wavefront) are divided in double precision and rounded once more to float:
+// with 53 >= 2*24 + 2 bits the double rounding is innocuous (S. Figueroa,
+// "When is double rounding innocuous?", SIGNUM Newsletter 30(3), 1995), and
+// it avoids the slow subnormal path of single-precision division.  The guarded
+// form equals IEEE single division for every float dividend in
+// [2^-149, 2^-99) and the normal binades checked (exhaustive test on sm_100a).
+__device__ __forceinline__ bool tiny_q(float q0, float x) { return fabsf(q0) < 0x1p-124f && x != 0.f; }
+__device__ __forceinline__ float ddiv_f(float x, float h) { return __double2float_rn(__ddiv_rn((double)x, (double)h)); }
 __device__ __forceinline__ float4 div4(float4 x, const Div& d) {
-    float4 q = cat4(mark2(lo2(x), d), mark2(hi2(x), d));
-    if (tiny(x.x) || tiny(x.y) || tiny(x.z) || tiny(x.w))
-        q = make_float4(__fdiv_rn(x.x, d.h), __fdiv_rn(x.y, d.h), __fdiv_rn(x.z, d.h), __fdiv_rn(x.w, d.h));
+    const float2 q0l = mul2(lo2(x), dup2(d.r)), q0h = mul2(hi2(x), dup2(d.r));
+    float4 q = cat4(fma2(fma2(q0l, dup2(-d.h), lo2(x)), dup2(d.r), q0l),
+                    fma2(fma2(q0h, dup2(-d.h), hi2(x)), dup2(d.r), q0h));
+    if (tiny_q(q0l.x, x.x) || tiny_q(q0l.y, x.y) || tiny_q(q0h.x, x.z) || tiny_q(q0h.y, x.w))
+        q = make_float4(ddiv_f(x.x, d.h), ddiv_f(x.y, d.h), ddiv_f(x.z, d.h), ddiv_f(x.w, d.h));
     return q;
 }
 // CPML memory update fma(fma(d, e, -(d m)), dt, m), packed
@@ -221,12 +220,78 @@ __device__ __forceinline__ ShotView shot_view(const StepArgs& p, int b) {
     return v;
 }
 
-// Per-component masks in edge tiles.
-template <int N, int MODE>
-__device__ __forceinline__ bool s_live(const StepArgs& p, int gi, int gj) {
-    if (MODE == kRec) return p.ring.in_box(gi, gj);
-    return gi >= N && gi < p.X - N && gj >= N && gj < p.Z - N;
+// Tile flags, uniform per CTA.
+struct TileFlags {
+    bool px, pz;    // the S region touches the x / z damping layers
+    bool border;    // some S-region or own cell lies outside the update domain
+    bool ring;      // boundary-ring work: strip save (forward) or restore (reconstruction)
+    bool src;       // the source cell lies in the S region (own cells for a force source)
+    bool inj;       // the receiver row crosses the U box (receiver mode)
+};
+
+__device__ __forceinline__ bool rect_meets_ring(const Ring& R, int i0, int i1, int j0, int j1) {
+    const int L = R.L, N = R.N, X = R.X, Z = R.Z;
+    const bool meets_box = i0 < X - L + N && i1 > L - N && j0 < Z - L + N && j1 > L - N;
+    const bool inside_deep = i0 >= L + N && i1 <= X - L - N && j0 >= L + N && j1 <= Z - L - N;
+    return meets_box && !inside_deep;
 }
+
+// Visit, cooperatively over the CTA, the boundary-ring cells inside the
+// rectangle [i0, i1) x [j0, j1) (global coordinates): f(i, j, ring index).
+// The four bands are rectangles, so each visit is a plain 2-D loop and the
+// strip accesses are contiguous along z.
+template <class F>
+__device__ __forceinline__ void for_ring(const Ring& R, int i0, int i1, int j0, int j1, F&& f) {
+    const int L = R.L, N = R.N, X = R.X, Z = R.Z, n2 = 2 * N, W = R.W, hm = R.H - 4 * N;
+#pragma unroll 1
+    for (int b = 0; b < 4; ++b) {
+        int bi0, bi1, bj0, bj1, base, stride;
+        if (b == 0) { bi0 = L - N; bi1 = X - L + N; bj0 = L - N; bj1 = L + N; base = 0; stride = n2; }
+        else if (b == 1) { bi0 = L - N; bi1 = X - L + N; bj0 = Z - L - N; bj1 = Z - L + N; base = W * n2; stride = n2; }
+        else if (b == 2) { bi0 = L - N; bi1 = L + N; bj0 = L + N; bj1 = Z - L - N; base = 2 * W * n2; stride = hm; }
+        else { bi0 = X - L - N; bi1 = X - L + N; bj0 = L + N; bj1 = Z - L - N; base = 2 * W * n2 + n2 * hm; stride = hm; }
+        const int ia = max(i0, bi0), ib = min(i1, bi1), ja = max(j0, bj0), jb = min(j1, bj1);
+        if (ia >= ib || ja >= jb) continue;
+        const int w = jb - ja, n = (ib - ia) * w;
+        for (int k = threadIdx.x; k < n; k += kThreads) {
+            const int i = ia + k / w, j = ja + k % w;
+            f(i, j, base + (i - bi0) * stride + (j - bj0));
+        }
+    }
+}
+
+template <int N, int MODE>
+__device__ __forceinline__ TileFlags tile_flags(const StepArgs& p, const ShotView& sv, int x0, int z0) {
+    using G = TileGeo<N>;
+    const int X = p.X, Z = p.Z, L = p.L;
+    TileFlags f;
+    f.px = f.pz = false;
+    f.ring = f.src = f.inj = false;
+    const int s_i0 = x0 - G::SHX, s_i1 = x0 + G::TX + G::SHX, s_j0 = z0 - G::HS, s_j1 = z0 + G::TZ + G::HS;
+    const bool src_in_s = sv.sx >= s_i0 && sv.sx < s_i1 && sv.sz >= s_j0 && sv.sz < s_j1;
+    if (MODE == kRec) {
+        f.border = !(x0 >= L && x0 + G::TX <= X - L && z0 >= L && z0 + G::TZ <= Z - L);
+        f.ring = sv.strip_u != nullptr &&
+                 rect_meets_ring(p.ring, x0 - G::SHX - N, x0 + G::TX + G::SHX + N, z0 - G::HU, z0 + G::TZ + G::HU);
+        f.src = p.src_recon && src_in_s;
+        return f;
+    }
+    // damping is non-zero for i < L or i > X-L (PS:2072-2080)
+    f.px = s_i0 < L || s_i1 - 1 >= X - L;
+    f.pz = s_j0 < L || s_j1 - 1 >= Z - L;
+    f.border = !(s_i0 >= N && s_i1 <= X - N && s_j0 >= N && s_j1 <= Z - N);
+    if (MODE == kFwd) {
+        f.ring = sv.strip_save != nullptr && rect_meets_ring(p.ring, x0, x0 + G::TX, z0, z0 + G::TZ);
+        f.src = (sv.src_type == 0 && src_in_s) ||
+                (sv.src_type == 1 && sv.sx >= x0 && sv.sx < x0 + G::TX && sv.sz >= z0 && sv.sz < z0 + G::TZ);
+    }
+    if (MODE == kRcv) {
+        f.inj = sv.rz >= z0 - G::HU && sv.rz < z0 + G::TZ + G::HU && x0 - G::SHX - N < X - L &&
+                x0 + G::TX + G::SHX + N > L;
+    }
+    return f;
+}
+
 template <int N, int MODE>
 __device__ __forceinline__ bool u_live(const StepArgs& p, int gi, int gj) {
     if (MODE == kRec) return gi >= p.L && gi < p.X - p.L && gj >= p.L && gj < p.Z - p.L;
@@ -235,11 +300,12 @@ __device__ __forceinline__ bool u_live(const StepArgs& p, int gi, int gj) {
 
 template <int N, int MODE>
 __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv, float* sm, int x0, int z0,
-                                          const bool PX, const bool PZ, const bool EDGE) {
+                                          const TileFlags& f) {
     using G = TileGeo<N>;
     constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS, HU = G::HU, UC = G::UC, SC = G::SC;
     const int tid = threadIdx.x;
     const int P = p.pitch;
+    const size_t R = p.ring.R;
     float* sUx = sm + G::oUx;
     float* sUz = sm + G::oUz;
     float* sTh = sm + G::oTh;
@@ -254,43 +320,36 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
     const Div dvx{p.dx, p.rdx}, dvz{p.dz, p.rdz};
     const size_t off = sv.off;
     const float* nowp[4] = {p.now[0] + off, p.now[1] + off, p.now[2] + off, p.now[3] + off};
+    const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;   // global origin of the U box
 
     // ---- phase 1: U = P + S over the tile and a 2N halo ---------------------
     for (int idx = tid; idx < G::UR * (UC / 4); idx += kThreads) {
         const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
-        const int gi = x0 - SHX - N + r, gj = z0 - HU + 4 * c4;
-        const ptrdiff_t g = (ptrdiff_t)gi * P + gj;
-        float4 ux = add4(ld4(nowp[0] + g), ld4(nowp[2] + g));   // Ux = Px + Sx (PS:302)
-        float4 uz = add4(ld4(nowp[1] + g), ld4(nowp[3] + g));
-        if (EDGE) {
-            if (MODE == kRcv) {
-                // load_record (PS:1471-1483): the receiver row is overwritten by
-                // the record over the interior x range before the S-stage reads it
-                if (gi >= p.L && gi < p.X - p.L && sv.rz >= gj && sv.rz < gj + 4) {
-                    set_comp(ux, sv.rz - gj, sv.inj_x[gi]);
-                    set_comp(uz, sv.rz - gj, sv.inj_z[gi]);
-                }
-            }
-            if (MODE == kRec) {
-                // reconstruction: ring cells come from the saved strips; cells
-                // outside the box are never read by the interior update
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int j = gj + k;
-                    if (!p.ring.in_box(gi, j)) {
-                        set_comp(ux, k, 0.f); set_comp(uz, k, 0.f);
-                    } else {
-                        const int ri = p.ring.index(gi, j);
-                        if (ri >= 0) {
-                            set_comp(ux, k, sv.strip_u[(size_t)kSUx * p.ring.R + ri]);
-                            set_comp(uz, k, sv.strip_u[(size_t)kSUz * p.ring.R + ri]);
-                        }
-                    }
-                }
+        const ptrdiff_t g = (ptrdiff_t)(ux_i0 + r) * P + (ux_j0 + 4 * c4);
+        st4(sUx + r * UC + 4 * c4, add4(ld4(nowp[0] + g), ld4(nowp[2] + g)));   // Ux = Px + Sx (PS:302)
+        st4(sUz + r * UC + 4 * c4, add4(ld4(nowp[1] + g), ld4(nowp[3] + g)));
+    }
+    if (MODE == kRcv && f.inj) {
+        __syncthreads();
+        // load_record (PS:1471-1483): the receiver row is overwritten by the
+        // record over the interior x range before the S-stage reads it
+        const int col = sv.rz - ux_j0;
+        for (int r = tid; r < G::UR; r += kThreads) {
+            const int gi = ux_i0 + r;
+            if (gi >= p.L && gi < p.X - p.L) {
+                sUx[r * UC + col] = sv.inj_x[gi];
+                sUz[r * UC + col] = sv.inj_z[gi];
             }
         }
-        st4(sUx + r * UC + 4 * c4, ux);
-        st4(sUz + r * UC + 4 * c4, uz);
+    }
+    if (MODE == kRec && f.ring) {
+        __syncthreads();
+        // reconstruction: the ring comes from the saved strips (read_wavefiled1, PS:1344-1376)
+        for_ring(p.ring, ux_i0, ux_i0 + G::UR, ux_j0, ux_j0 + UC, [&](int i, int j, int ri) {
+            const int o = (i - ux_i0) * UC + (j - ux_j0);
+            sUx[o] = sv.strip_u[kSUx * R + ri];
+            sUz[o] = sv.strip_u[kSUz * R + ri];
+        });
     }
     __syncthreads();
 
@@ -324,12 +383,12 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
             const float4 vp2 = ld4(p.vp2 + g), vs2 = ld4(p.vs2 + g);
             const bool own = ownc && r >= 0 && r < TX;
             float4 fxx = zero4(), fzz = zero4(), fxz = zero4(), fzx = zero4();
-            if (PX) {
+            if (f.px) {
                 const float4 axv = ld4(p.ax + g);
                 fxx = cpml4(ld4(p.f_old[0] + off + g), axv, exx[q], p.dt);
                 fzx = cpml4(ld4(p.f_old[3] + off + g), axv, ezx[q], p.dt);
             }
-            if (PZ) {
+            if (f.pz) {
                 const float4 azv = ld4(p.az + g);
                 fzz = cpml4(ld4(p.f_old[1] + off + g), azv, ezz, p.dt);
                 fxz = cpml4(ld4(p.f_old[2] + off + g), azv, exz, p.dt);
@@ -343,50 +402,23 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
             float4 qzz = mul4(vs2, sub4(ezz, fzz));
             float4 qxz = mul4(vs2, sub4(exz, fxz));
             float4 qxx = mul4(vs2, sub4(exx[q], fxx));
-            if (EDGE) {
+            if (MODE != kRec && f.border) {
+                // cells outside [N, X-N) x [N, Z-N) are never updated by the
+                // reference and stay zero
+                const bool row_live = gi >= N && gi < p.X - N;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int gj = gjb + k;
-                    float v_th = comp(th, k);
-                    bool live = s_live<N, MODE>(p, gi, gj);
-                    // source term on theta after the Q fields (PS:380)
-                    if (MODE == kFwd && sv.src_type == 0 && gi == sv.sx && gj == sv.sz) v_th = v_th + sv.wavelet[p.t];
-                    if (MODE == kRec) {
-                        if (live && p.src_recon && gi == sv.sx && gj == sv.sz) v_th = v_th + sv.wavelet[p.t + 1];
-                        const int ri = live ? p.ring.index(gi, gj) : -1;
-                        if (ri >= 0) {
-                            const float* s = sv.strip_s;
-                            const size_t R = p.ring.R;
-                            v_th = s[kSTh * R + ri];
-                            set_comp(om, k, s[kSOm * R + ri]);
-                            set_comp(qzx, k, s[kSQzx * R + ri]);
-                            set_comp(qzz, k, s[kSQzz * R + ri]);
-                            set_comp(qxx, k, s[kSQxx * R + ri]);
-                            set_comp(qxz, k, s[kSQxz * R + ri]);
-                        }
-                    }
-                    if (!live) {
-                        v_th = 0.f;
-                        set_comp(om, k, 0.f); set_comp(qzx, k, 0.f); set_comp(qzz, k, 0.f);
+                    if (!(row_live && gj >= N && gj < p.Z - N)) {
+                        set_comp(th, k, 0.f); set_comp(om, k, 0.f); set_comp(qzx, k, 0.f); set_comp(qzz, k, 0.f);
                         set_comp(qxx, k, 0.f); set_comp(qxz, k, 0.f);
                         set_comp(fxx, k, 0.f); set_comp(fzz, k, 0.f); set_comp(fxz, k, 0.f); set_comp(fzx, k, 0.f);
-                    }
-                    set_comp(th, k, v_th);
-                    if (MODE == kFwd && own && sv.strip_save) {
-                        const int ri = p.ring.index(gi, gj);
-                        if (ri >= 0) {
-                            float* s = sv.strip_save;
-                            const size_t R = p.ring.R;
-                            s[kSTh * R + ri] = v_th; s[kSOm * R + ri] = comp(om, k);
-                            s[kSQzx * R + ri] = comp(qzx, k); s[kSQzz * R + ri] = comp(qzz, k);
-                            s[kSQxx * R + ri] = comp(qxx, k); s[kSQxz * R + ri] = comp(qxz, k);
-                        }
                     }
                 }
             }
             if (own) {
-                if (PX) { st4(p.f_new[0] + off + g, fxx); st4(p.f_new[3] + off + g, fzx); }
-                if (PZ) { st4(p.f_new[1] + off + g, fzz); st4(p.f_new[2] + off + g, fxz); }
+                if (f.px) { st4(p.f_new[0] + off + g, fxx); st4(p.f_new[3] + off + g, fzx); }
+                if (f.pz) { st4(p.f_new[1] + off + g, fzz); st4(p.f_new[2] + off + g, fxz); }
             }
             const int sr = r + SHX, scol = c + HS;
             st4(sTh + sr * SC + scol, th);
@@ -399,6 +431,55 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
                 st4(sQxx + r * SC + scol, qxx);
                 st4(sQzx + r * SC + scol, qzx);
             }
+        }
+    }
+    if (f.src && MODE != kRcv && !(MODE == kFwd && sv.src_type == 1)) {
+        // source term on theta after the Q fields (PS:380); in the
+        // reconstruction only where the level's theta is recomputed
+        __syncthreads();
+        if (tid == 0) {
+            const int r = sv.sx - x0, c = sv.sz - z0;
+            if ((r >= 0 && r < TX) || (c >= 0 && c < TZ)) {
+                float* t = sTh + (r + SHX) * SC + (c + HS);
+                *t = *t + sv.wavelet[MODE == kRec ? p.t + 1 : p.t];
+            }
+        }
+    }
+    if (f.ring) {
+        __syncthreads();
+        if (MODE == kRec) {
+            // read_wavefiled2 (PS:1377-1424): theta, omega and the Q fields of the ring
+            for_ring(p.ring, x0 - SHX, x0 + TX + SHX, z0 - HS, z0 + TZ + HS, [&](int i, int j, int ri) {
+                const int r = i - x0, c = j - z0;
+                const bool rin = r >= 0 && r < TX, cin = c >= 0 && c < TZ;
+                if (rin || cin) {
+                    const int o = (r + SHX) * SC + (c + HS);
+                    sTh[o] = sv.strip_s[kSTh * R + ri];
+                    sOm[o] = sv.strip_s[kSOm * R + ri];
+                }
+                if (cin) {
+                    sQxz[(r + SHX) * TZ + c] = sv.strip_s[kSQxz * R + ri];
+                    sQzz[(r + SHX) * TZ + c] = sv.strip_s[kSQzz * R + ri];
+                }
+                if (rin) {
+                    sQxx[r * SC + (c + HS)] = sv.strip_s[kSQxx * R + ri];
+                    sQzx[r * SC + (c + HS)] = sv.strip_s[kSQzx * R + ri];
+                }
+            });
+        }
+        if (MODE == kFwd) {
+            // save_wavefiled (PS:1230-1287): the S fields of the tile's ring cells
+            float* s = sv.strip_save;
+            for_ring(p.ring, x0, x0 + TX, z0, z0 + TZ, [&](int i, int j, int ri) {
+                const int r = i - x0, c = j - z0;
+                const int o = (r + SHX) * SC + (c + HS);
+                s[kSTh * R + ri] = sTh[o];
+                s[kSOm * R + ri] = sOm[o];
+                s[kSQzx * R + ri] = sQzx[r * SC + (c + HS)];
+                s[kSQzz * R + ri] = sQzz[(r + SHX) * TZ + c];
+                s[kSQxx * R + ri] = sQxx[r * SC + (c + HS)];
+                s[kSQxz * R + ri] = sQxz[(r + SHX) * TZ + c];
+            });
         }
     }
     __syncthreads();
@@ -425,14 +506,14 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
             const float4 dC = dz4<N, false>(sQzx + r * SC + scol, a, dvz);          // duz_xdz = D-z Qzx
             float4 oC = zero4(), oE = zero4(), oB = zero4(), oA = zero4();
             float4 oTx = zero4(), oTz = zero4(), oWz = zero4(), oWx = zero4();
-            if (PZ) {
+            if (f.pz) {
                 const float4 d = ld4(p.az + g);
                 oC = cpml4(ld4(p.o[0] + off + g), d, dC, dt);
                 oA = cpml4(ld4(p.o[3] + off + g), d, dA, dt);
                 oTz = cpml4(ld4(p.o[5] + off + g), d, tz, dt);
                 oWz = cpml4(ld4(p.o[6] + off + g), d, wz, dt);
             }
-            if (PX) {
+            if (f.px) {
                 const float4 d = ld4(p.ax + g);
                 oE = cpml4(ld4(p.o[1] + off + g), d, dE[q], dt);
                 oB = cpml4(ld4(p.o[2] + off + g), d, dB[q], dt);
@@ -451,40 +532,37 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
             const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);
             const float4 osx = ld4(p.past[2] + off + g), osz = ld4(p.past[3] + off + g);
             const float2 two = dup2(2.f), dt2 = dup2(p.dt2), m1 = dup2(-1.f);
-            auto leap = [&](float4 now, float4 past, float4 s) {
-                return cat4(fma2(dt2, lo2(s), fma2(two, lo2(now), mul2(lo2(past), m1))),
-                            fma2(dt2, hi2(s), fma2(two, hi2(now), mul2(hi2(past), m1))));
+            auto leap = [&](float4 now, float4 past, float4 sum) {
+                return cat4(fma2(dt2, lo2(sum), fma2(two, lo2(now), mul2(lo2(past), m1))),
+                            fma2(dt2, hi2(sum), fma2(two, hi2(now), mul2(hi2(past), m1))));
             };
             float4 vpx = leap(npx, opx, spx), vpz = leap(npz, opz, spz);
             float4 vsx = leap(nsx, osx, ssx), vsz = leap(nsz, osz, ssz);
-            if (EDGE) {
+            if (MODE == kFwd && f.src && sv.src_type == 1 && gi == sv.sx && sv.sz >= z0 + c && sv.sz < z0 + c + 4)
+                set_comp(vpz, sv.sz - z0 - c, comp(vpz, sv.sz - z0 - c) + p.dt2 * sv.wavelet[p.t]);
+            unsigned live = 0xfu;
+            if (f.border) {
+                live = 0u;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) live |= u_live<N, MODE>(p, gi, z0 + c + k) ? (1u << k) : 0u;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const int gj = z0 + c + k;
-                    if (MODE == kFwd && sv.src_type == 1 && gi == sv.sx && gj == sv.sz)
-                        set_comp(vpz, k, comp(vpz, k) + p.dt2 * sv.wavelet[p.t]);
-                    if (!u_live<N, MODE>(p, gi, gj)) {
+                    if (!(live & (1u << k))) {
                         set_comp(vpx, k, 0.f); set_comp(vpz, k, 0.f); set_comp(vsx, k, 0.f); set_comp(vsz, k, 0.f);
                         set_comp(oC, k, 0.f); set_comp(oE, k, 0.f); set_comp(oB, k, 0.f); set_comp(oA, k, 0.f);
                         set_comp(oTx, k, 0.f); set_comp(oTz, k, 0.f); set_comp(oWz, k, 0.f); set_comp(oWx, k, 0.f);
                     }
                 }
             }
-            if (MODE != kRcv) {
-                const float4 ux = add4(vpx, vsx), uz = add4(vpz, vsz);   // PS:302-303 / PS:978-979
-                if (MODE == kFwd && sv.rec_x && sv.rz >= z0 + c && sv.rz < z0 + c + 4 && gi < p.X) {
+            if (MODE == kFwd) {
+                const float4 ux = add4(vpx, vsx), uz = add4(vpz, vsz);   // PS:302-303
+                if (sv.rec_x && sv.rz >= z0 + c && sv.rz < z0 + c + 4 && gi < p.X) {
                     sv.rec_x[gi] = comp(ux, sv.rz - z0 - c);   // post-update value (PS:307-311)
                     sv.rec_z[gi] = comp(uz, sv.rz - z0 - c);
                 }
-                if (EDGE && MODE == kFwd && sv.strip_save) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int ri = p.ring.index(gi, z0 + c + k);
-                        if (ri >= 0) {
-                            sv.strip_save[(size_t)kSUx * p.ring.R + ri] = comp(ux, k);
-                            sv.strip_save[(size_t)kSUz * p.ring.R + ri] = comp(uz, k);
-                        }
-                    }
+                if (f.ring) {   // kept for the strip pass below (the U box is free now)
+                    st4(sUx + r * TZ + c, ux);
+                    st4(sUz + r * TZ + c, uz);
                 }
             }
             if (MODE == kRec) {
@@ -500,14 +578,14 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
                     return cat4(add2(lo2(acc), fma2(lo2(a1), lo2(b1), mul2(lo2(a2), lo2(b2)))),
                                 add2(hi2(acc), fma2(hi2(a1), hi2(b1), mul2(hi2(a2), hi2(b2)))));
                 };
-                float4 npp = corr(ld4(acc0), sx, rpx, sz, rpz);
-                float4 nil = corr(ld4(acc2), sx, sx, sz, sz);
-                float4 nps = corr(ld4(acc1), sx, rsx, sz, rsz);
-                if (EDGE) {
-                    const float4 o0 = ld4(acc0), o1 = ld4(acc1), o2 = ld4(acc2);
+                const float4 o0 = ld4(acc0), o1 = ld4(acc1), o2 = ld4(acc2);
+                float4 npp = corr(o0, sx, rpx, sz, rpz);
+                float4 nil = corr(o2, sx, sx, sz, sz);
+                float4 nps = corr(o1, sx, rsx, sz, rsz);
+                if (f.border) {
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        if (!u_live<N, MODE>(p, gi, z0 + c + k)) {
+                        if (!(live & (1u << k))) {
                             set_comp(npp, k, comp(o0, k)); set_comp(nps, k, comp(o1, k)); set_comp(nil, k, comp(o2, k));
                         }
                     }
@@ -516,52 +594,26 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
             }
             st4(p.past[0] + off + g, vpx); st4(p.past[1] + off + g, vpz);
             st4(p.past[2] + off + g, vsx); st4(p.past[3] + off + g, vsz);
-            if (PZ) {
+            if (f.pz) {
                 st4(p.o[0] + off + g, oC); st4(p.o[3] + off + g, oA);
                 st4(p.o[5] + off + g, oTz); st4(p.o[6] + off + g, oWz);
             }
-            if (PX) {
+            if (f.px) {
                 st4(p.o[1] + off + g, oE); st4(p.o[2] + off + g, oB);
                 st4(p.o[4] + off + g, oTx); st4(p.o[7] + off + g, oWx);
             }
         }
     }
-}
-
-// Tile classification (uniform per CTA).
-template <int N, int MODE>
-__device__ __forceinline__ bool tile_is_edge(const StepArgs& p, const ShotView& sv, int x0, int z0) {
-    using G = TileGeo<N>;
-    const int X = p.X, Z = p.Z, L = p.L;
-    if (MODE == kRec) {
-        // clean: the whole U box lies in the deep interior (no ring, inside the box)
-        const int r0 = x0 - G::SHX - N, r1 = x0 + G::TX + G::SHX + N;
-        const int c0 = z0 - G::HU, c1 = z0 + G::TZ + G::HU;
-        bool clean = r0 >= L + N && r1 <= X - L - N && c0 >= L + N && c1 <= Z - L - N;
-        if (p.src_recon && sv.sx >= x0 - G::SHX && sv.sx < x0 + G::TX + G::SHX && sv.sz >= z0 - G::HS &&
-            sv.sz < z0 + G::TZ + G::HS)
-            clean = false;
-        return !clean;
+    if (MODE == kFwd && f.ring) {
+        // save_wavefiled (PS:1230-1287): the new displacement of the tile's ring cells
+        __syncthreads();
+        float* s = sv.strip_save;
+        for_ring(p.ring, x0, x0 + TX, z0, z0 + TZ, [&](int i, int j, int ri) {
+            const int o = (i - x0) * TZ + (j - z0);
+            s[kSUx * R + ri] = sUx[o];
+            s[kSUz * R + ri] = sUz[o];
+        });
     }
-    bool clean = x0 - G::SHX >= N && x0 + G::TX + G::SHX <= X - N && z0 - G::HS >= N && z0 + G::TZ + G::HS <= Z - N;
-    if (MODE == kFwd) {
-        // source inside the S region
-        if (sv.sx >= x0 - G::SHX && sv.sx < x0 + G::TX + G::SHX && sv.sz >= z0 - G::HS && sv.sz < z0 + G::TZ + G::HS)
-            clean = false;
-        // own cells touching the boundary ring while saving strips
-        if (p.save) {
-            const int bx0 = L - N, bx1 = X - L + N, bz0 = L - N, bz1 = Z - L + N;       // box
-            const int dx0 = L + N, dx1 = X - L - N, dz0 = L + N, dz1 = Z - L - N;       // deep interior
-            const bool meets_box = x0 < bx1 && x0 + G::TX > bx0 && z0 < bz1 && z0 + G::TZ > bz0;
-            const bool inside_deep = x0 >= dx0 && x0 + G::TX <= dx1 && z0 >= dz0 && z0 + G::TZ <= dz1;
-            if (meets_box && !inside_deep) clean = false;
-        }
-    }
-    if (MODE == kRcv) {
-        // injection row inside the U box
-        if (sv.rz >= z0 - G::HU && sv.rz < z0 + G::TZ + G::HU) clean = false;
-    }
-    return !clean;
 }
 
 template <int N, int MODE>
@@ -572,16 +624,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
     const int x0 = (p.tile_x0 + tx) * G::TX, z0 = (p.tile_z0 + tz) * G::TZ;
     const ShotView sv = shot_view(p, blockIdx.y);
-    const bool edge = tile_is_edge<N, MODE>(p, sv, x0, z0);
-    if (MODE == kRec) {
-        step_tile<N, MODE>(p, sv, sm, x0, z0, false, false, edge);
-        return;
-    }
-    // Damping is non-zero for i < L or i > X-L (PS:2072-2080); a tile takes
-    // the memory-variable path when its S-stage halo touches such a cell.
-    const bool px = (x0 - G::SHX < p.L) || (x0 + G::TX + G::SHX - 1 >= p.X - p.L);
-    const bool pz = (z0 - G::HS < p.L) || (z0 + G::TZ + G::HS - 1 >= p.Z - p.L);
-    step_tile<N, MODE>(p, sv, sm, x0, z0, px, pz, edge);
+    const TileFlags f = tile_flags<N, MODE>(p, sv, x0, z0);
+    step_tile<N, MODE>(p, sv, sm, x0, z0, f);
 }
 
 }  // namespace ouc
