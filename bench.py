@@ -281,7 +281,7 @@ def main():
     abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg)) * B
     achieved = abytes / (per_launch_ms / 1e3) / 1e9
     tr = committed_traffic()
-    traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name else None
+    traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name and tr.get("batch") == B else None
 
     if rank == 0:
         cpu = None
