@@ -41,7 +41,8 @@ enum {
     OUC_EUNSTABLE = 4,   /* CFL limit exceeded or non-finite wavefield          */
     OUC_ESTATE = 5,      /* call out of order (e.g. stack before any shot)      */
     OUC_ETIMEOUT = 6,    /* a bounded device wait ran out                       */
-    OUC_ENODEV = 7       /* no usable sm_100 device                             */
+    OUC_ENODEV = 7,      /* no usable sm_100 device                             */
+    OUC_ESCRATCH = 8     /* problem larger than the fixed scratch of ouc_forward_noalloc */
 };
 
 enum { OUC_MODEL_INTERIOR = 0, OUC_MODEL_PADDED = 1 };
@@ -164,6 +165,27 @@ int ouc_rtm_batch_dev(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const flo
  * Any output may be NULL; reset != 0 clears the stack after reading. */
 int ouc_stack(ouc_ctx* ctx, double* stack_pp, double* stack_ps, double* illum, int reset);
 int ouc_stack_dev(ouc_ctx* ctx, const double** d_pp, const double** d_ps, const double** d_illum);
+
+/* Forward modeling that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory when they need
+ * a modeling run: applications whose own memory pool owns the whole GPU and
+ * forbids other allocations, and pipelines that reserve memory up front and
+ * must not enter the allocator later (cudaMalloc/cudaFree synchronise the
+ * device and can fail under memory pressure).  Same kernels and results as
+ * ouc_forward; the wavefield state lives in a fixed library-owned device
+ * array of OUC_NOALLOC_SCRATCH_BYTES (held on each GPU that loads it until
+ * process exit).  Inputs and outputs are the caller's device buffers:
+ * d_vp, d_vs padded X*Z models (x-major), d_wavelet nt samples, gathers X*nt
+ * each in cfg->gather_layout.  Work is queued on cfg->stream and the call
+ * returns without synchronising.  The first call on a device looks up the
+ * array's address: make it before any stream capture on that device.  All
+ * calls share the array and it keeps the last call's contents (each call
+ * clears what it needs zeroed); calls whose work overlaps on the GPU race, so
+ * serialise them.  Sizes beyond the array return OUC_ESCRATCH; the CFL check
+ * of ouc_create is the caller's responsibility here. */
+#define OUC_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, const float* d_vp, const float* d_vs,
+                        const float* d_wavelet, float* d_gather_vx, float* d_gather_vz);
 
 #ifdef __cplusplus
 }

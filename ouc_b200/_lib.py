@@ -12,7 +12,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libouc.so")
 
-OUC_OK, OUC_EINVAL, OUC_ECUDA, OUC_ENOMEM, OUC_EUNSTABLE, OUC_ESTATE, OUC_ETIMEOUT, OUC_ENODEV = range(8)
+OUC_OK, OUC_EINVAL, OUC_ECUDA, OUC_ENOMEM, OUC_EUNSTABLE, OUC_ESTATE, OUC_ETIMEOUT, OUC_ENODEV, OUC_ESCRATCH = range(9)
 
 
 class ouc_config(C.Structure):
@@ -58,6 +58,7 @@ SIGNATURES = {
                                 C.POINTER(_fp), C.POINTER(_fp)]),
     "ouc_rtm_batch_dev": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), _vp, C.POINTER(_vp), C.POINTER(_vp),
                                     C.POINTER(_vp), C.POINTER(_vp)]),
+    "ouc_forward_noalloc": (C.c_int, [C.POINTER(ouc_config), C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
     "ouc_stack": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
     "ouc_stack_dev": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
 }

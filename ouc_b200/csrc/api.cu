@@ -374,6 +374,7 @@ const char* ouc_strerror(int status) {
         case OUC_ESTATE: return "call out of order";
         case OUC_ETIMEOUT: return "device wait timed out";
         case OUC_ENODEV: return "no usable sm_100 device";
+        case OUC_ESCRATCH: return "problem larger than the fixed scratch of the no-allocation entry point";
     }
     return "unknown status";
 }
