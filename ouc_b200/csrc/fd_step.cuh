@@ -489,15 +489,17 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
         const int rr = 2 * (tid / (TZ / 4));
         const int c = 4 * (tid % (TZ / 4));
         const int scol = c + HS;
-        float4 tx[2], wx[2], dB[2], dE[2];
-        dx4<N, 2, true>(sTh + (rr + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
-        dx4<N, 2, false>(sOm + (rr + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
-        dx4<N, 2, false>(sQxz + (rr + SHX) * TZ + c, TZ, a, dvx, dB);     // dux_zdx = D-x Qxz
-        dx4<N, 2, true>(sQzz + (rr + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
         const float dt = p.dt;
-#pragma unroll
+        // a rolled two-iteration loop: half the code of an unrolled pair of
+        // rows, which keeps the hot path inside the instruction cache
+#pragma unroll 1
         for (int q = 0; q < 2; ++q) {
             const int r = rr + q;
+            float4 tx[1], wx[1], dB[1], dE[1];
+            dx4<N, 1, true>(sTh + (r + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
+            dx4<N, 1, false>(sOm + (r + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
+            dx4<N, 1, false>(sQxz + (r + SHX) * TZ + c, TZ, a, dvx, dB);     // dux_zdx = D-x Qxz
+            dx4<N, 1, true>(sQzz + (r + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
             const int gi = x0 + r;
             const ptrdiff_t g = (ptrdiff_t)gi * P + (z0 + c);
             const float4 tz = dz4<N, true>(sTh + (r + SHX) * SC + scol, a, dvz);    // dthetadz
@@ -515,18 +517,18 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
             }
             if (f.px) {
                 const float4 d = ld4(p.ax + g);
-                oE = cpml4(ld4(p.o[1] + off + g), d, dE[q], dt);
-                oB = cpml4(ld4(p.o[2] + off + g), d, dB[q], dt);
-                oTx = cpml4(ld4(p.o[4] + off + g), d, tx[q], dt);
-                oWx = cpml4(ld4(p.o[7] + off + g), d, wx[q], dt);
+                oE = cpml4(ld4(p.o[1] + off + g), d, dE[0], dt);
+                oB = cpml4(ld4(p.o[2] + off + g), d, dB[0], dt);
+                oTx = cpml4(ld4(p.o[4] + off + g), d, tx[0], dt);
+                oWx = cpml4(ld4(p.o[7] + off + g), d, wx[0], dt);
             }
             // leapfrog brackets in the reference's order (PS:291-294); zero
             // memories outside the damping layers change no rounding
-            const float4 nwx = make_float4(-wx[q].x, -wx[q].y, -wx[q].z, -wx[q].w);
-            const float4 spx = add4(sub4(sub4(add4(sub4(tx[q], oTx), dC), dE[q]), oC), oE);
-            const float4 spz = add4(sub4(sub4(add4(sub4(tz, oTz), dB[q]), dA), oB), oA);
-            const float4 ssx = add4(sub4(sub4(add4(sub4(wz, oWz), dC), dE[q]), oC), oE);
-            const float4 ssz = add4(sub4(sub4(add4(add4(nwx, oWx), dB[q]), dA), oB), oA);
+            const float4 nwx = make_float4(-wx[0].x, -wx[0].y, -wx[0].z, -wx[0].w);
+            const float4 spx = add4(sub4(sub4(add4(sub4(tx[0], oTx), dC), dE[0]), oC), oE);
+            const float4 spz = add4(sub4(sub4(add4(sub4(tz, oTz), dB[0]), dA), oB), oA);
+            const float4 ssx = add4(sub4(sub4(add4(sub4(wz, oWz), dC), dE[0]), oC), oE);
+            const float4 ssz = add4(sub4(sub4(add4(add4(nwx, oWx), dB[0]), dA), oB), oA);
             const float4 npx = ld4(nowp[0] + g), npz = ld4(nowp[1] + g);
             const float4 nsx = ld4(nowp[2] + g), nsz = ld4(nowp[3] + g);
             const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);
