@@ -249,11 +249,13 @@ def main():
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     if world > 1:
-        stk = torch.zeros(3 * cfg.nx * cfg.nz, dtype=torch.float64, device="cuda")
         tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-        dist.all_reduce(stk)   # the cross-shot FP64 stack exchange
+        # the cross-shot exchange: sum of the ranks' FP64 stacks (PP, PS, illumination)
+        from ouc_b200 import survey
+        stk = [torch.from_numpy(a).cuda() for a in mig.stack(reset=True)]
+        survey.reduce_stack(*stk)
         dist.barrier()
     clk = clocks.stop()
     cells = w.cell_updates_per_shot() * B

@@ -166,6 +166,41 @@ int ouc_rtm_batch_dev(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const flo
 int ouc_stack(ouc_ctx* ctx, double* stack_pp, double* stack_ps, double* illum, int reset);
 int ouc_stack_dev(ouc_ctx* ctx, const double** d_pp, const double** d_ps, const double** d_illum);
 
+/* Step-level interface: one RTM shot advanced one reference time step per
+ * call, for comparing against the reference's kernels step by step.  The
+ * calls must come in the order of the reference's main():
+ *   ouc_step_begin                once: zero both wavefields and the imaging
+ *                                 accumulators, take the wavelet and, if
+ *                                 given, the observed records (host arrays,
+ *                                 cfg.gather_layout; NULL: the forward steps
+ *                                 record them, PS:307-311);
+ *   ouc_step_forward(t)           t = 0 .. nt-1: forward_s + forward_u +
+ *                                 record + save_wavefiled (PS:2261-2266); the
+ *                                 last one also mutes the records when the
+ *                                 shot asks for it (PS:2296-2297);
+ *   ouc_step_receiver(t)          t = nt-1 .. 0: load_record + rt_s_res +
+ *                                 rt_u_res (PS:2319-2324, 2349-2354);
+ *   ouc_step_reconstruct(t)       after ouc_step_receiver(t): reshot_u,
+ *                                 read_wavefiled1, reshot_s, read_wavefiled2
+ *                                 and corr_v (PS:2326-2361);
+ *   ouc_image_finalize            image_fun + Laplace (PS:2365-2376) into
+ *                                 img_pp / img_ps (host, nx*nz, may be NULL),
+ *                                 and the FP64 stack.
+ * A call out of this order returns OUC_ESTATE and changes nothing.  Results
+ * equal ouc_rtm_shot's bit for bit.  A whole-shot call (ouc_forward*,
+ * ouc_rtm_*) ends a stepped shot.  ouc_step_fields copies the current
+ * displacement of one wavefield (side 0 = source, 1 = receiver) to the host
+ * as 6 padded X*Z arrays: Ux, Uz, Px, Pz, Sx, Sz (PS:291-303); during the
+ * backward steps the source side holds the reconstructed wavefield, which
+ * is defined on the interior only. */
+int ouc_step_begin(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rec_vx,
+                   const float* rec_vz);
+int ouc_step_forward(ouc_ctx* ctx, int t);
+int ouc_step_receiver(ouc_ctx* ctx, int t);
+int ouc_step_reconstruct(ouc_ctx* ctx, int t);
+int ouc_image_finalize(ouc_ctx* ctx, float* img_pp, float* img_ps);
+int ouc_step_fields(ouc_ctx* ctx, int side, float* fields);
+
 /* Forward modeling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they need
  * a modeling run: applications whose own memory pool owns the whole GPU and

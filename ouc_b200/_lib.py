@@ -61,6 +61,12 @@ SIGNATURES = {
     "ouc_forward_noalloc": (C.c_int, [C.POINTER(ouc_config), C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
     "ouc_stack": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
     "ouc_stack_dev": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
+    "ouc_step_begin": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp]),
+    "ouc_step_forward": (C.c_int, [_vp, C.c_int]),
+    "ouc_step_receiver": (C.c_int, [_vp, C.c_int]),
+    "ouc_step_reconstruct": (C.c_int, [_vp, C.c_int]),
+    "ouc_image_finalize": (C.c_int, [_vp, _fp, _fp]),
+    "ouc_step_fields": (C.c_int, [_vp, C.c_int, _fp]),
 }
 
 _lib = None

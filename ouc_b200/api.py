@@ -231,6 +231,45 @@ class Context:
         sc = shot.c()
         check(lib().ouc_forward_dev(self._h, C.byref(sc), d_wavelet, d_gx, d_gz), self._h)
 
+    # -- step-level interface: one RTM shot, one reference time step per call
+    def step_begin(self, shot: Shot, wavelet, recs=None):
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        rx = rz = None
+        if recs is not None:
+            rx, rz = _f32(recs[0]), _f32(recs[1])
+            assert rx.shape == self._gshape() and rz.shape == self._gshape()
+        sc = shot.c()
+        check(lib().ouc_step_begin(self._h, C.byref(sc), _p(w), _p(rx), _p(rz)), self._h)
+
+    def step_forward(self, t):
+        check(lib().ouc_step_forward(self._h, int(t)), self._h)
+
+    def step_receiver(self, t):
+        check(lib().ouc_step_receiver(self._h, int(t)), self._h)
+
+    def step_reconstruct(self, t):
+        check(lib().ouc_step_reconstruct(self._h, int(t)), self._h)
+
+    def image_finalize(self):
+        pp = np.zeros((self.cfg.nx, self.cfg.nz), np.float32)
+        ps = np.zeros_like(pp)
+        check(lib().ouc_image_finalize(self._h, _p(pp), _p(ps)), self._h)
+        return pp, ps
+
+    def step_fields(self, side=0):
+        """(6, X, Z): Ux, Uz, Px, Pz, Sx, Sz of the source (0) or receiver (1) side."""
+        f = np.zeros((6, self.X, self.Z), np.float32)
+        check(lib().ouc_step_fields(self._h, int(side), _p(f)), self._h)
+        return f
+
+    def stack_dev(self):
+        """Device addresses of the context's FP64 stacks (PP, PS, illumination),
+        each nx x nz, x-major; valid until the context is closed."""
+        p = [C.c_void_p(), C.c_void_p(), C.c_void_p()]
+        check(lib().ouc_stack_dev(self._h, C.byref(p[0]), C.byref(p[1]), C.byref(p[2])), self._h)
+        return tuple(q.value for q in p)
+
     def stack(self, reset=False):
         n = (self.cfg.nx, self.cfg.nz)
         pp, ps, il = np.zeros(n), np.zeros(n), np.zeros(n)

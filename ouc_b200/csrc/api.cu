@@ -89,6 +89,12 @@ struct ouc_ctx {
     size_t bytes = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
+    // step-level interface: one shot (slot 0) advanced one launch per call
+    enum { kIdle, kForward, kReceiver, kReconstruct, kFinalize } step_phase = kIdle;
+    int step_t = 0;              // the time the next step call must name
+    ouc_shot step_shot{};
+    StepArgs step_fwd{}, step_rcv{}, step_rec{};
+
     float* field(float* base, size_t k) const { return base + k * fstride + (size_t)kGX * pitch + kZOFF; }
     float* gather(int b, int comp) const { return gathers + ((size_t)b * 2 + comp) * (size_t)nt * X; }
 };
@@ -237,6 +243,18 @@ int zero_side(ouc_ctx* ctx, int n, int side, bool with_acc) {
     return OUC_OK;
 }
 
+// One forward step of n shots at time t (forward_s + forward_u with the
+// receiver record and the strip save, PS:2261-2266); `a` carries record/save.
+int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t) {
+    bind_side(a, s);
+    a.t = t;
+    if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+    s.swap_levels();
+    s.swap_memory();
+    ctx->timing.kernel_launches += 1;
+    return OUC_OK;
+}
+
 // Forward time loop (PS:2258-2292) of n shots.  Records into the time-major
 // gathers when `record`, saves the boundary ring of every step when `save`.
 int run_forward(ouc_ctx* ctx, int n, bool record, bool save) {
@@ -246,16 +264,60 @@ int run_forward(ouc_ctx* ctx, int n, bool record, bool save) {
     StepArgs a = base_args(ctx);
     a.record = record;
     a.save = save;
-    for (int t = 0; t < ctx->nt; ++t) {
-        bind_side(a, s);
-        a.t = t;
-        if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
-        s.swap_levels();
-        s.swap_memory();
-    }
+    for (int t = 0; t < ctx->nt; ++t)
+        if ((rc = fwd_step(ctx, a, s, n, t))) return rc;
     ctx->src = s;
-    ctx->timing.kernel_launches += ctx->nt;
     CK(cudaGetLastError());
+    return OUC_OK;
+}
+
+// Launch arguments of the two backward wavefields.
+StepArgs rcv_args(const ouc_ctx* ctx) { return base_args(ctx); }
+
+StepArgs rec_args(const ouc_ctx* ctx) {
+    StepArgs as = base_args(ctx);
+    as.tiles_z = ctx->rec_tiles_z; as.tile_x0 = ctx->rec_tx0; as.tile_z0 = ctx->rec_tz0;
+    as.img_past = ctx->cfg.image_align == OUC_IMAGE_REFERENCE;
+    for (int k = 0; k < 3; ++k) as.acc[k] = ctx->acc[k];
+    return as;
+}
+
+// Receiver side at time t: record injection + S/U stages with damping
+// (PS:2319-2324, 2349-2354).
+int rcv_step(ouc_ctx* ctx, StepArgs& ar, Side& r, int n, int t) {
+    bind_side(ar, r);
+    ar.t = t;
+    if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+    r.swap_levels();
+    r.swap_memory();
+    ctx->timing.kernel_launches += 1;
+    return OUC_OK;
+}
+
+// Source side at time t, after rcv_step(t): inverse leapfrog on the interior
+// from levels t+1 and t+2 with the strip restore, and the imaging condition
+// (PS:2326-2361).  At t = nt-1 there is no reconstruction: the forward's
+// final level is correlated as it stands.
+int rec_step(ouc_ctx* ctx, StepArgs& as, Side& s, const Side& r, int n, int t, bool exact_strips, bool theta_src) {
+    const int nt = ctx->nt;
+    if (t == nt - 1) {
+        StepArgs ai = base_args(ctx);
+        for (int k = 0; k < 4; ++k) { ai.now[k] = s.now[k]; ai.rcv[k] = r.now[k]; }
+        for (int k = 0; k < 3; ++k) ai.acc[k] = ctx->acc[k];
+        launch_image_only(ai, n, ctx->stream);
+        ctx->timing.kernel_launches += 1;
+        s.swap_levels();   // now = level NT-1, past = level NT
+        return OUC_OK;
+    }
+    bind_side(as, s);
+    as.t = t;
+    as.src_recon = theta_src && (exact_strips || t + 1 == nt - 1);
+    as.slot_u = exact_strips ? t : (t + 1 == nt - 1 ? nt - 2 : t + 1);
+    as.slot_s = t + 1;
+    for (int k = 0; k < 4; ++k) as.rcv[k] = r.now[k];
+    if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+    s.swap_levels();
+    ctx->timing.kernel_launches += 1;
     return OUC_OK;
 }
 
@@ -264,45 +326,14 @@ int run_forward(ouc_ctx* ctx, int n, bool record, bool save) {
 int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
     Side s = ctx->src;
     Side r = ctx->rcv;
-    const int nt = ctx->nt;
     int rc = zero_side(ctx, n, 1, true);
     if (rc) return rc;
-    StepArgs ar = base_args(ctx);
-    StepArgs as = base_args(ctx);
-    as.tiles_z = ctx->rec_tiles_z; as.tile_x0 = ctx->rec_tx0; as.tile_z0 = ctx->rec_tz0;
-    as.img_past = ctx->cfg.image_align == OUC_IMAGE_REFERENCE;
-    for (int k = 0; k < 3; ++k) as.acc[k] = ctx->acc[k];
-    long long launches = 0;
-    for (int t = nt - 1; t >= 0; --t) {
-        // receiver side: injection + S/U stages with damping (PS:2319-2324, 2349-2354)
-        bind_side(ar, r);
-        ar.t = t;
-        if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
-        r.swap_levels();
-        r.swap_memory();
-        ++launches;
-        if (t == nt - 1) {
-            // no reconstruction at the last level: correlate the forward's final P
-            StepArgs ai = base_args(ctx);
-            for (int k = 0; k < 4; ++k) { ai.now[k] = s.now[k]; ai.rcv[k] = r.now[k]; }
-            for (int k = 0; k < 3; ++k) ai.acc[k] = ctx->acc[k];
-            launch_image_only(ai, n, ctx->stream);
-            ++launches;
-            s.swap_levels();   // now = level NT-1, past = level NT
-            continue;
-        }
-        // source side: inverse leapfrog on the interior from levels t+1 and t+2
-        bind_side(as, s);
-        as.t = t;
-        as.src_recon = theta_src && (exact_strips || t + 1 == nt - 1);
-        as.slot_u = exact_strips ? t : (t + 1 == nt - 1 ? nt - 2 : t + 1);
-        as.slot_s = t + 1;
-        for (int k = 0; k < 4; ++k) as.rcv[k] = r.now[k];
-        if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
-        s.swap_levels();
-        ++launches;
+    StepArgs ar = rcv_args(ctx);
+    StepArgs as = rec_args(ctx);
+    for (int t = ctx->nt - 1; t >= 0; --t) {
+        if ((rc = rcv_step(ctx, ar, r, n, t))) return rc;
+        if ((rc = rec_step(ctx, as, s, r, n, t, exact_strips, theta_src))) return rc;
     }
-    ctx->timing.kernel_launches += launches;
     CK(cudaGetLastError());
     return OUC_OK;
 }
@@ -581,6 +612,7 @@ static int forward_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet
     if (rc) return rc;
     if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
     cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;   // whole-shot calls overwrite any stepped state
     ctx->timing = ouc_timing{};
     const float* d_w = wavelet;
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
@@ -675,6 +707,7 @@ static int rtm_batch_impl(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const
     for (int b = 0; b < nshots; ++b)
         if ((rc = check_shot(ctx, &shots[b]))) return rc;
     cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;   // whole-shot calls overwrite any stepped state
     if ((rc = ensure_strips(ctx))) return rc;
     ctx->timing = ouc_timing{};
     const float* d_w = wavelet;
@@ -730,6 +763,127 @@ int ouc_stack_dev(ouc_ctx* ctx, const double** pp, const double** ps, const doub
     if (pp) *pp = ctx->d_stack[0];
     if (ps) *ps = ctx->d_stack[1];
     if (illum) *illum = ctx->d_stack[2];
+    return OUC_OK;
+}
+
+// ---- step-level interface -------------------------------------------------
+
+static int step_order(ouc_ctx* ctx, int phase, int t) {
+    if (ctx->step_phase != phase || t != ctx->step_t) {
+        static const char* names[] = {"ouc_step_begin", "ouc_step_forward", "ouc_step_receiver",
+                                      "ouc_step_reconstruct", "ouc_image_finalize"};
+        const char* want = names[ctx->step_phase];
+        return fail(ctx, OUC_ESTATE, std::string("step call out of order: expected ") + want +
+                                         (ctx->step_phase == ouc_ctx::kIdle || ctx->step_phase == ouc_ctx::kFinalize
+                                              ? std::string()
+                                              : " at t = " + std::to_string(ctx->step_t)));
+    }
+    cudaSetDevice(ctx->device);
+    return OUC_OK;
+}
+
+int ouc_step_begin(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, const float* rec_vx,
+                   const float* rec_vz) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = check_shot(ctx, shot);
+    if (rc) return rc;
+    if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
+    if ((rec_vx == nullptr) != (rec_vz == nullptr)) return fail(ctx, OUC_EINVAL, "give both record components or neither");
+    cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;
+    if ((rc = ensure_strips(ctx))) return rc;
+    ctx->timing = ouc_timing{};
+    CK(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = upload_desc(ctx, 1, shot, ctx->d_wavelet))) return rc;
+    if ((rc = zero_side(ctx, 1, 0, false)) || (rc = zero_side(ctx, 1, 1, true))) return rc;
+    if (rec_vx) {
+        if ((rc = gather_in(ctx, rec_vx, ctx->gather(0, 0), true))) return rc;
+        if ((rc = gather_in(ctx, rec_vz, ctx->gather(0, 1), true))) return rc;
+    }
+    ctx->step_shot = *shot;
+    ctx->step_fwd = base_args(ctx);
+    ctx->step_fwd.record = rec_vx == nullptr;
+    ctx->step_fwd.save = 1;
+    ctx->step_rcv = rcv_args(ctx);
+    ctx->step_rec = rec_args(ctx);
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->step_phase = ouc_ctx::kForward;
+    ctx->step_t = 0;
+    return OUC_OK;
+}
+
+int ouc_step_forward(ouc_ctx* ctx, int t) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = step_order(ctx, ouc_ctx::kForward, t);
+    if (rc || (rc = fwd_step(ctx, ctx->step_fwd, ctx->src, 1, t))) return rc;
+    CK(cudaGetLastError());
+    if (++ctx->step_t < ctx->nt) return OUC_OK;
+    // forward done: mute the records as the whole-shot path does (PS:2296-2297)
+    const ouc_shot& sh = ctx->step_shot;
+    if (sh.mute) {
+        const int sx = sh.sx + ctx->L, sz = sh.sz + ctx->L, rzz = sh.rz + ctx->L;
+        launch_mute(ctx->gather(0, 0), ctx->gather(0, 1), ctx->X, ctx->nt, sx, sz, rzz, sh.t0, ctx->cfg.dt,
+                    ctx->cfg.dx, ctx->vp_host[(size_t)sx * ctx->Z + rzz], ctx->stream);
+        ctx->timing.kernel_launches += 1;
+    }
+    ctx->step_phase = ouc_ctx::kReceiver;
+    ctx->step_t = ctx->nt - 1;
+    return OUC_OK;
+}
+
+int ouc_step_receiver(ouc_ctx* ctx, int t) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = step_order(ctx, ouc_ctx::kReceiver, t);
+    if (rc || (rc = rcv_step(ctx, ctx->step_rcv, ctx->rcv, 1, t))) return rc;
+    CK(cudaGetLastError());
+    ctx->step_phase = ouc_ctx::kReconstruct;
+    return OUC_OK;
+}
+
+int ouc_step_reconstruct(ouc_ctx* ctx, int t) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = step_order(ctx, ouc_ctx::kReconstruct, t);
+    if (rc) return rc;
+    rc = rec_step(ctx, ctx->step_rec, ctx->src, ctx->rcv, 1, t, ctx->cfg.strip_level == OUC_STRIP_EXACT,
+                  ctx->step_shot.src_type == OUC_SRC_THETA);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    if (--ctx->step_t >= 0) {
+        ctx->step_phase = ouc_ctx::kReceiver;
+    } else {
+        ctx->step_phase = ouc_ctx::kFinalize;
+        ctx->step_t = 0;
+    }
+    return OUC_OK;
+}
+
+int ouc_image_finalize(ouc_ctx* ctx, float* img_pp, float* img_ps) {
+    if (!ctx) return OUC_EINVAL;
+    int rc = step_order(ctx, ouc_ctx::kFinalize, 0);
+    if (rc || (rc = finalize(ctx, 1))) return rc;
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    if (img_pp) CK(cudaMemcpyAsync(img_pp, ctx->d_img, ni * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (img_ps) CK(cudaMemcpyAsync(img_ps, ctx->d_img + ni, ni * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->step_phase = ouc_ctx::kIdle;
+    return OUC_OK;
+}
+
+int ouc_step_fields(ouc_ctx* ctx, int side, float* fields) {
+    if (!ctx) return OUC_EINVAL;
+    if (!fields || (side != 0 && side != 1)) return fail(ctx, OUC_EINVAL, "fields is NULL or side is not 0/1");
+    if (ctx->step_phase == ouc_ctx::kIdle) return fail(ctx, OUC_ESTATE, "no shot is being stepped");
+    cudaSetDevice(ctx->device);
+    const Side& s = side == 0 ? ctx->src : ctx->rcv;
+    const float* f[4] = {s.now[0], s.now[1], s.now[2], s.now[3]};
+    launch_pack_fields(f, 4, ctx->X, ctx->Z, ctx->pitch, ctx->staging, ctx->stream);
+    const size_t C = (size_t)ctx->X * ctx->Z;
+    CK(cudaMemcpyAsync(fields + 2 * C, ctx->staging, 4 * C * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t k = 0; k < C; ++k) {
+        fields[k] = fields[2 * C + k] + fields[4 * C + k];       // Ux = Px + Sx (PS:302)
+        fields[C + k] = fields[3 * C + k] + fields[5 * C + k];   // Uz = Pz + Sz (PS:303)
+    }
     return OUC_OK;
 }
 
