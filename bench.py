@@ -179,6 +179,12 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=None, help="CPU sample length (time steps)")
     ap.add_argument("--batch", type=int, default=16, help="shots advanced together per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--strips", default="fp32", choices=["fp32", "fp16", "bf16"],
+                    help="boundary-strip storage (fp16: scaled per slot and field)")
+    ap.add_argument("--compensated", action="store_true", help="compensated FP32 imaging sums")
+    ap.add_argument("--snapshot-every", type=int, default=0,
+                    help="0: reconstruct the source wavefield from boundary strips (the reference's method); "
+                         "K: store source snapshots every K imaging levels instead (--strips sets their storage)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -212,6 +218,9 @@ def main():
     records = [true_ctx.forward(s, wavelet)[:2] for s in my_shots]
     true_ctx.close()
     cfg.max_batch = B
+    cfg.strip_precision = {"fp32": o.PREC_FP32, "fp16": o.PREC_FP16, "bf16": o.PREC_BF16}[args.strips]
+    cfg.compensated_image = int(args.compensated)
+    cfg.snapshot_every = args.snapshot_every
     mig = o.Context(cfg, w.vp_mig, w.vs_mig, w.rho)
     stream = torch.cuda.ExternalStream(mig.stream, device=torch.device("cuda", local))
 
@@ -258,7 +267,9 @@ def main():
         survey.reduce_stack(*stk)
         dist.barrier()
     clk = clocks.stop()
-    cells = w.cell_updates_per_shot() * B
+    # cell-updates actually performed: forward + receiver on the padded grid,
+    # plus the reconstruction on the interior when the strips form runs it
+    cells = (w.cell_updates_per_shot() if not args.snapshot_every else 2 * cfg.nt * cfg.X * cfg.Z) * B
     value = cells * args.steps * world / (ms / 1e3) / 1e9
     shots_per_hour = 3600.0 * B * args.steps * world / (ms / 1e3)
 
@@ -280,7 +291,7 @@ def main():
     # roofline of the dominant kernel: the fused forward step (k_step, forward mode)
     peak, peak_kind = measured_peak()
     per_launch_ms = statistics.median(fwd_ms) / nt
-    abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg)) * B
+    abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg), 4 if args.strips == "fp32" else 2) * B
     achieved = abytes / (per_launch_ms / 1e3) / 1e9
     tr = committed_traffic()
     traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name and tr.get("batch") == B else None
@@ -296,6 +307,9 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model, modelled records)",
             "config": {"workload": w.name, "grid": [cfg.X, cfg.Z], "interior": [cfg.nx, cfg.nz], "nt": nt,
                        "half_order": cfg.half_order, "dx_m": cfg.dx, "dt_s": cfg.dt, "step": f"one batch of {B} RTM shots advanced together", "batch": B,
+                       "strips": args.strips, "compensated_image": bool(args.compensated),
+                       "source_wavefield": (f"snapshots every {args.snapshot_every} imaging levels" if args.snapshot_every
+                                            else "reconstructed from boundary strips"),
                        "l2": "256 MiB buffer written between timed shots; 3.8 GB of boundary strips per shot",
                        "parallelism": f"shots sharded over {world} GPU(s)"},
             "shots_per_hour": shots_per_hour,

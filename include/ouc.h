@@ -74,12 +74,20 @@ typedef struct ouc_config {
     int model_layout;       /* OUC_MODEL_INTERIOR or OUC_MODEL_PADDED            */
     int strip_level;        /* OUC_STRIP_*                                       */
     int image_align;        /* OUC_IMAGE_*                                       */
-    int strip_precision;    /* OUC_PREC_*: storage of the boundary strips        */
+    int strip_precision;    /* OUC_PREC_*: storage of the saved source wavefield
+                               (boundary strips, or the snapshots below); FP16 is
+                               scaled by a power of two per slot and field      */
     int compensated_image;  /* 1: compensated-FP32 per-shot accumulators         */
     int gather_layout;      /* OUC_GATHER_*                                      */
     int device;             /* CUDA device ordinal                               */
     void* stream;           /* cudaStream_t to run on, or NULL for a private one */
     int max_batch;          /* shots advanced together per launch (0 or 1: one)  */
+    int snapshot_every;     /* 0: rebuild the source wavefield backwards from the
+                               boundary strips (the reference's method, PS:2326-
+                               2361); K >= 1: store the source P wavefield of
+                               every K-th imaging level during the forward pass
+                               and image only those levels (no reconstruction;
+                               no counterpart in the reference)                 */
 } ouc_config;
 
 typedef struct ouc_shot {

@@ -44,6 +44,7 @@ class Config:
     device: int = 0
     stream: int = 0
     max_batch: int = 1
+    snapshot_every: int = 0     # 0: strips + reconstruction; K: source snapshots every K imaging levels
 
     def c(self):
         c = _lib.ouc_config()

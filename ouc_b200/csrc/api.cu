@@ -23,6 +23,10 @@
 
 using namespace ouc;
 
+static_assert((int)OUC_PREC_FP32 == (int)ouc::kStripF32 && (int)OUC_PREC_FP16 == (int)ouc::kStripF16 &&
+                  (int)OUC_PREC_BF16 == (int)ouc::kStripBF16,
+              "strip precision codes");
+
 namespace {
 
 // Float32 staggered weights.  N = 6: the reference's literals (PS:221).
@@ -39,7 +43,7 @@ const double kWeights[7][6] = {
 };
 
 constexpr int kFieldsPerSide = 24;                    // now 4, past 4, F old 4, F new 4, O 8
-constexpr int kFieldsPerShot = 2 * kFieldsPerSide + 3;   // source side, receiver side, accumulators
+constexpr int kFieldsPerShot = 2 * kFieldsPerSide + 6;   // source side, receiver side, accumulators + compensation
 
 // Field pointers of one wavefield (shot 0 of the batch).
 struct Side {
@@ -78,12 +82,21 @@ struct ouc_ctx {
     float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
     Side src{}, rcv{};
     float* acc[3] = {nullptr, nullptr, nullptr};
+    float* comp[3] = {nullptr, nullptr, nullptr};   // compensation terms of acc (compensated_image)
     float* gathers = nullptr;    // [batch][2][nt][X], time-major
     float* staging = nullptr;    // max(nt*X, 4*X*Z) floats for transposes / packing
     float* d_wavelet = nullptr;
     float* d_img = nullptr;      // [batch][2][nx][nz]
     double* d_stack[3] = {nullptr, nullptr, nullptr};
-    float* strips = nullptr;     // [batch][nt][8][R]
+    void* strips = nullptr;      // [batch][nt][8][R] of the strip element type
+    float* stage = nullptr;      // f16 strips: staging rings [batch][2][8][R]
+    unsigned* amax = nullptr;    // f16 strips: per-slot field maxima [batch][nt][8]
+    // snapshot form (cfg.snapshot_every = K >= 1)
+    void* snaps = nullptr;       // [batch][nslots][2][nx][nz] of the strip element type
+    unsigned* snap_amax = nullptr;   // f16: [batch][nslots][2]
+    int nslots = 0;
+    std::vector<int> snap_fwd;   // forward step -> snapshot slot of its new level, or -1
+    std::vector<int> snap_bwd;   // backward step -> slot imaged there, or -1
     size_t strip_slot = 0;       // floats per slot
     ShotDesc* d_desc = nullptr;  // [batch]
     size_t bytes = 0;
@@ -176,6 +189,9 @@ StepArgs base_args(const ouc_ctx* c) {
     a.vp2 = c->vp2; a.vs2 = c->vs2; a.ax = c->ax; a.az = c->az;
     a.shot_stride = c->shot_stride;
     a.strip_slot = c->strip_slot;
+    a.strip_prec = c->cfg.strip_precision;
+    a.comp_image = c->cfg.compensated_image;
+    for (int k = 0; k < 3; ++k) a.comp[k] = c->comp[k];
     a.ring = c->ring;
     a.shots = c->d_desc;
     return a;
@@ -201,15 +217,54 @@ int check_shot(ouc_ctx* ctx, const ouc_shot* s) {
 
 int ensure_strips(ouc_ctx* ctx) {
     if (ctx->strips) return OUC_OK;
-    const size_t bytes = ctx->strip_slot * (size_t)ctx->nt * ctx->batch * sizeof(float);
-    cudaError_t e = cudaMalloc(&ctx->strips, bytes);
-    if (e != cudaSuccess) {
-        ctx->strips = nullptr;
+    const int prec = ctx->cfg.strip_precision;
+    const size_t bytes = ctx->strip_slot * (size_t)ctx->nt * ctx->batch * strip_elem_bytes(prec);
+    const size_t stage = prec == kStripF16 ? ctx->strip_slot * 2 * ctx->batch * sizeof(float) : 0;
+    const size_t amax = prec == kStripF16 ? (size_t)ctx->nt * kStripFields * ctx->batch * sizeof(unsigned) : 0;
+    bool ok = cudaMalloc(&ctx->strips, bytes) == cudaSuccess;
+    if (ok && stage) ok = cudaMalloc(&ctx->stage, stage) == cudaSuccess && cudaMalloc(&ctx->amax, amax) == cudaSuccess;
+    if (!ok) {
         cudaGetLastError();
-        return fail(ctx, OUC_ENOMEM, "cannot allocate boundary strips (" + std::to_string(bytes >> 20) + " MiB)");
+        cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
+        ctx->strips = nullptr; ctx->stage = nullptr; ctx->amax = nullptr;
+        return fail(ctx, OUC_ENOMEM, "cannot allocate boundary strips (" + std::to_string((bytes + stage) >> 20) + " MiB)");
     }
-    ctx->bytes += bytes;
+    ctx->bytes += bytes + stage + amax;
     return OUC_OK;
+}
+
+int ensure_snaps(ouc_ctx* ctx) {
+    if (ctx->snaps) return OUC_OK;
+    const int prec = ctx->cfg.strip_precision;
+    const size_t elems = (size_t)ctx->nslots * 2 * ctx->nx * ctx->nz * ctx->batch;
+    const size_t bytes = elems * strip_elem_bytes(prec);
+    const size_t amax = prec == kStripF16 ? (size_t)ctx->nslots * 2 * ctx->batch * sizeof(unsigned) : 0;
+    bool ok = cudaMalloc(&ctx->snaps, bytes) == cudaSuccess;
+    if (ok && amax) ok = cudaMalloc(&ctx->snap_amax, amax) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
+        ctx->snaps = nullptr; ctx->snap_amax = nullptr;
+        return fail(ctx, OUC_ENOMEM, "cannot allocate source snapshots (" + std::to_string(bytes >> 20) + " MiB)");
+    }
+    ctx->bytes += bytes + amax;
+    return OUC_OK;
+}
+
+SnapArgs snap_args(const ouc_ctx* ctx, int slot) {
+    SnapArgs a;
+    memset(&a, 0, sizeof(a));
+    a.X = ctx->X; a.Z = ctx->Z; a.pitch = ctx->pitch; a.L = ctx->L; a.nx = ctx->nx; a.nz = ctx->nz;
+    a.shot_stride = ctx->shot_stride;
+    a.prec = ctx->cfg.strip_precision;
+    a.slot = slot;
+    a.nslots = ctx->nslots;
+    a.shot_elems = (size_t)ctx->nslots * 2 * ctx->nx * ctx->nz;
+    a.snaps = ctx->snaps;
+    a.amax = ctx->snap_amax;
+    a.comp_image = ctx->cfg.compensated_image;
+    for (int k = 0; k < 3; ++k) { a.acc[k] = ctx->acc[k]; a.comp[k] = ctx->comp[k]; }
+    return a;
 }
 
 // Upload the descriptors of n shots (padded coordinates).
@@ -223,7 +278,11 @@ int upload_desc(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_wavel
         d[b].wavelet = d_wavelet;
         d[b].gather_x = ctx->gather(b, 0);
         d[b].gather_z = ctx->gather(b, 1);
-        d[b].strips = ctx->strips ? ctx->strips + (size_t)b * ctx->nt * ctx->strip_slot : nullptr;
+        d[b].strips = ctx->strips ? static_cast<char*>(ctx->strips) + (size_t)b * ctx->nt * ctx->strip_slot *
+                                                                   strip_elem_bytes(ctx->cfg.strip_precision)
+                                  : nullptr;
+        d[b].stage = ctx->stage ? ctx->stage + (size_t)b * 2 * ctx->strip_slot : nullptr;
+        d[b].amax = ctx->amax ? ctx->amax + (size_t)b * ctx->nt * kStripFields : nullptr;
     }
     CK(cudaMemcpyAsync(ctx->d_desc, d.data(), n * sizeof(ShotDesc), cudaMemcpyHostToDevice, ctx->stream));
     return OUC_OK;
@@ -237,7 +296,7 @@ int zero_side(ouc_ctx* ctx, int n, int side, bool with_acc) {
         CK(cudaMemsetAsync(base, 0, (size_t)kFieldsPerSide * ctx->fstride * sizeof(float), ctx->stream));
         if (with_acc) {
             float* acc = ctx->state + (size_t)b * ctx->shot_stride + (size_t)2 * kFieldsPerSide * ctx->fstride;
-            CK(cudaMemsetAsync(acc, 0, (size_t)3 * ctx->fstride * sizeof(float), ctx->stream));
+            CK(cudaMemsetAsync(acc, 0, (size_t)6 * ctx->fstride * sizeof(float), ctx->stream));   // acc + comp
         }
     }
     return OUC_OK;
@@ -257,15 +316,31 @@ int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t) {
 
 // Forward time loop (PS:2258-2292) of n shots.  Records into the time-major
 // gathers when `record`, saves the boundary ring of every step when `save`.
-int run_forward(ouc_ctx* ctx, int n, bool record, bool save) {
+int run_forward(ouc_ctx* ctx, int n, bool record, bool save, bool snaps = false) {
     Side s = ctx->src;
     int rc = zero_side(ctx, n, 0, false);
     if (rc) return rc;
     StepArgs a = base_args(ctx);
     a.record = record;
     a.save = save;
-    for (int t = 0; t < ctx->nt; ++t)
+    const bool f16 = save && ctx->cfg.strip_precision == kStripF16;
+    if (f16) CK(cudaMemsetAsync(ctx->amax, 0, (size_t)n * ctx->nt * kStripFields * sizeof(unsigned), ctx->stream));
+    if (snaps && ctx->snap_amax)
+        CK(cudaMemsetAsync(ctx->snap_amax, 0, (size_t)n * ctx->nslots * 2 * sizeof(unsigned), ctx->stream));
+    for (int t = 0; t < ctx->nt; ++t) {
         if ((rc = fwd_step(ctx, a, s, n, t))) return rc;
+        if (snaps && ctx->snap_fwd[t] >= 0) {   // the new level is an imaging level: keep it
+            SnapArgs sa = snap_args(ctx, ctx->snap_fwd[t]);
+            sa.px = s.now[0];
+            sa.pz = s.now[1];
+            launch_snap_store(sa, n, ctx->stream);
+            ctx->timing.kernel_launches += ctx->snap_amax ? 2 : 1;
+        }
+    }
+    if (f16) {   // the last slot: its maxima are complete now
+        launch_strip_pack(ctx->d_desc, n, ctx->nt - 1, ctx->ring.R, ctx->strip_slot, ctx->stream);
+        ctx->timing.kernel_launches += 1;
+    }
     ctx->src = s;
     CK(cudaGetLastError());
     return OUC_OK;
@@ -338,13 +413,38 @@ int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
     return OUC_OK;
 }
 
+// Backward loop of the snapshot form: receiver back-propagation at every
+// step, imaging at the snapshot levels only.
+int run_backward_snap(ouc_ctx* ctx, int n) {
+    Side r = ctx->rcv;
+    int rc = zero_side(ctx, n, 1, true);
+    if (rc) return rc;
+    StepArgs ar = rcv_args(ctx);
+    for (int t = ctx->nt - 1; t >= 0; --t) {
+        if ((rc = rcv_step(ctx, ar, r, n, t))) return rc;
+        if (ctx->snap_bwd[t] >= 0) {
+            SnapArgs sa = snap_args(ctx, ctx->snap_bwd[t]);
+            for (int k = 0; k < 4; ++k) sa.rcv[k] = r.now[k];
+            launch_image_snap(sa, n, ctx->stream);
+            ctx->timing.kernel_launches += 1;
+        }
+    }
+    CK(cudaGetLastError());
+    return OUC_OK;
+}
+
 int finalize(ouc_ctx* ctx, int n) {
     FinalizeArgs f;
     f.X = ctx->X; f.Z = ctx->Z; f.pitch = ctx->pitch; f.L = ctx->L;
     f.nshots = n;
     f.shot_stride = ctx->shot_stride;
     f.dh = ctx->cfg.dx;   // main() passes dx as the Laplacian spacing (PS:2372)
-    for (int k = 0; k < 3; ++k) { f.acc[k] = ctx->acc[k]; f.stack[k] = ctx->d_stack[k]; }
+    f.illum_scale = ctx->cfg.snapshot_every > 0 ? ctx->cfg.snapshot_every : 1;
+    for (int k = 0; k < 3; ++k) {
+        f.acc[k] = ctx->acc[k];
+        f.comp[k] = ctx->cfg.compensated_image ? ctx->comp[k] : nullptr;
+        f.stack[k] = ctx->d_stack[k];
+    }
     f.img = ctx->d_img;
     launch_finalize(f, ctx->stream);
     ctx->timing.kernel_launches += 1;
@@ -457,6 +557,11 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     if (cfg->dx > 256.f || cfg->dz > 256.f) return bad("grid spacing above 256 is not supported");
     if (!(cfg->pml_r > 0 && cfg->pml_r < 1)) return bad("pml_r must be in (0, 1)");
     if (cfg->max_batch < 0 || cfg->max_batch > 256) return bad("max_batch must be in [0, 256]");
+    if (cfg->strip_precision != OUC_PREC_FP32 && cfg->strip_precision != OUC_PREC_FP16 &&
+        cfg->strip_precision != OUC_PREC_BF16)
+        return bad("strip_precision must be OUC_PREC_FP32, OUC_PREC_FP16 or OUC_PREC_BF16");
+    if (cfg->compensated_image != 0 && cfg->compensated_image != 1) return bad("compensated_image must be 0 or 1");
+    if (cfg->snapshot_every < 0 || cfg->snapshot_every > cfg->nt) return bad("snapshot_every must be in [0, nt]");
     ctx->N = N; ctx->L = L; ctx->nx = cfg->nx; ctx->nz = cfg->nz; ctx->nt = cfg->nt;
     ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
     ctx->batch = std::max(1, cfg->max_batch);
@@ -527,6 +632,20 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->rec_tiles_z = (Z - L - 1) / TZ - ctx->rec_tz0 + 1;
     ctx->ring = Ring::make(X, Z, L, N);
     ctx->strip_slot = (size_t)kStripFields * ctx->ring.R;
+    if (cfg->snapshot_every > 0) {
+        // imaging steps t = nt-1, nt-1-K, ...; step t correlates the source
+        // level t+1 (EXACT, and the last step) or t+2 (REFERENCE, PS:2361),
+        // i.e. the new level of forward step t or t+1: one slot per distinct
+        // forward step
+        const int K = cfg->snapshot_every, nt = cfg->nt;
+        ctx->snap_fwd.assign(nt, -1);
+        ctx->snap_bwd.assign(nt, -1);
+        for (int t = nt - 1; t >= 0; t -= K) {
+            const int f = (cfg->image_align == OUC_IMAGE_EXACT || t == nt - 1) ? t : t + 1;
+            if (ctx->snap_fwd[f] < 0) ctx->snap_fwd[f] = ctx->nslots++;
+            ctx->snap_bwd[t] = ctx->snap_fwd[f];
+        }
+    }
 
     const size_t model_bytes = 4 * ctx->fstride * sizeof(float);
     const size_t state_bytes = ctx->shot_stride * ctx->batch * sizeof(float);
@@ -563,6 +682,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         for (int q = 0; q < 8; ++q) s->o[q] = ctx->field(ctx->state, k++);
     }
     for (int q = 0; q < 3; ++q) ctx->acc[q] = ctx->field(ctx->state, k++);
+    for (int q = 0; q < 3; ++q) ctx->comp[q] = ctx->field(ctx->state, k++);
     int rc = OUC_OK;
     if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
         (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data()))) {
@@ -581,7 +701,8 @@ int ouc_destroy(ouc_ctx* ctx) {
     cudaFree(ctx->gathers); cudaFree(ctx->staging); cudaFree(ctx->d_wavelet);
     cudaFree(ctx->d_img); cudaFree(ctx->d_desc);
     for (auto* p : ctx->d_stack) cudaFree(p);
-    cudaFree(ctx->strips);
+    cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
+    cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -659,9 +780,10 @@ static int rtm_group(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_
                      const float* const* rz, float* const* ipp, float* const* ips, bool host) {
     int rc;
     const bool self_records = rx == nullptr;
+    const bool snap = ctx->cfg.snapshot_every > 0;
     if ((rc = upload_desc(ctx, n, shots, d_w))) return rc;
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    if ((rc = run_forward(ctx, n, self_records, true))) return rc;
+    if ((rc = run_forward(ctx, n, self_records, !snap, snap))) return rc;
     for (int b = 0; b < n && !self_records; ++b) {
         if (!rx[b] || !rz[b]) return fail(ctx, OUC_EINVAL, "record pointer missing for a shot");
         if ((rc = gather_in(ctx, rx[b], ctx->gather(b, 0), host))) return rc;
@@ -679,7 +801,8 @@ static int rtm_group(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_
     const bool theta = shots[0].src_type == OUC_SRC_THETA;
     for (int b = 1; b < n; ++b)
         if ((shots[b].src_type == OUC_SRC_THETA) != theta) return fail(ctx, OUC_EINVAL, "mixed source types in a batch");
-    if ((rc = run_backward(ctx, n, ctx->cfg.strip_level == OUC_STRIP_EXACT, theta))) return rc;
+    rc = snap ? run_backward_snap(ctx, n) : run_backward(ctx, n, ctx->cfg.strip_level == OUC_STRIP_EXACT, theta);
+    if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     if ((rc = finalize(ctx, n))) return rc;
     const size_t ni = (size_t)ctx->nx * ctx->nz;
@@ -708,7 +831,7 @@ static int rtm_batch_impl(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const
         if ((rc = check_shot(ctx, &shots[b]))) return rc;
     cudaSetDevice(ctx->device);
     ctx->step_phase = ouc_ctx::kIdle;   // whole-shot calls overwrite any stepped state
-    if ((rc = ensure_strips(ctx))) return rc;
+    if ((rc = ctx->cfg.snapshot_every > 0 ? ensure_snaps(ctx) : ensure_strips(ctx))) return rc;
     ctx->timing = ouc_timing{};
     const float* d_w = wavelet;
     if (host) {
@@ -789,6 +912,8 @@ int ouc_step_begin(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, con
     if (rc) return rc;
     if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
     if ((rec_vx == nullptr) != (rec_vz == nullptr)) return fail(ctx, OUC_EINVAL, "give both record components or neither");
+    if (ctx->cfg.snapshot_every > 0)
+        return fail(ctx, OUC_EINVAL, "the step-level calls follow the reconstruction form (snapshot_every = 0)");
     cudaSetDevice(ctx->device);
     ctx->step_phase = ouc_ctx::kIdle;
     if ((rc = ensure_strips(ctx))) return rc;

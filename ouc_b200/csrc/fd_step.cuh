@@ -40,6 +40,8 @@
 // IEEE division on sm_100a for the spacings in use); quotients near the
 // subnormal range go through double precision (div4 below).
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "ouc_internal.h"
@@ -198,9 +200,7 @@ struct ShotView {
     float* rec_z;
     const float* inj_x;    // gather row t (kRcv)
     const float* inj_z;
-    float* strip_save;     // kFwd: slot t
-    const float* strip_u;  // kRec: U slot
-    const float* strip_s;  // kRec: theta..Qxz slot
+    bool strips;           // the shot has boundary strips
     size_t off;            // state offset of this shot (floats)
 };
 
@@ -213,11 +213,71 @@ __device__ __forceinline__ ShotView shot_view(const StepArgs& p, int b) {
     v.rec_z = p.record ? d.gather_z + (size_t)p.t * p.X : nullptr;
     v.inj_x = d.gather_x + (size_t)p.t * p.X;
     v.inj_z = d.gather_z + (size_t)p.t * p.X;
-    v.strip_save = (p.save && d.strips) ? d.strips + (size_t)p.t * p.strip_slot : nullptr;
-    v.strip_u = d.strips ? d.strips + (size_t)p.slot_u * p.strip_slot : nullptr;
-    v.strip_s = d.strips ? d.strips + (size_t)p.slot_s * p.strip_slot : nullptr;
+    v.strips = d.strips != nullptr;
     v.off = (size_t)b * p.shot_stride;
     return v;
+}
+
+// ---- boundary-strip elements (StripPrec) -----------------------------------
+// Strip pointers are formed inside the ring passes from the shot descriptor,
+// so that they hold no registers through the rest of the step.
+
+// 2^k for k in [-126, 127]
+__device__ __forceinline__ float pow2f(int k) { return __int_as_float((k + 127) << 23); }
+
+// v * 2^k for k in [-252, 254], as two exact power-of-two multiplies
+__device__ __forceinline__ float scale2(float v, int k) {
+    const int k1 = k / 2;
+    return v * pow2f(k1) * pow2f(k - k1);
+}
+
+// kStripF16 scale exponent of a slot/field whose largest |v| has the bits
+// `a` (a non-negative float): that value maps into [2^14, 2^15), so every
+// scaled value is below 2^15 and converts to a finite half.
+__device__ __forceinline__ int f16_exp(unsigned a) {
+    if (a == 0) return 0;
+    const int e = (a >> 23) ? (int)(a >> 23) - 127 : (31 - __clz(a)) - 149;   // floor(log2 a)
+    return 14 - e;
+}
+
+__device__ __forceinline__ size_t slot_bytes(const StepArgs& p) {
+    return p.strip_slot * (size_t)strip_elem_bytes(p.strip_prec);
+}
+
+// Slot `slot` of a shot's strips (element type per p.strip_prec).
+__device__ __forceinline__ const void* strip_slot_ptr(const StepArgs& p, const ShotDesc& d, int slot) {
+    return static_cast<const char*>(d.strips) + (size_t)slot * slot_bytes(p);
+}
+
+__device__ __forceinline__ float strip_get(const StepArgs& p, const void* base, const unsigned* amax, int f, int idx) {
+    if (p.strip_prec == kStripF32) return static_cast<const float*>(base)[idx];
+    if (p.strip_prec == kStripBF16) return __bfloat162float(static_cast<const __nv_bfloat16*>(base)[idx]);
+    return scale2(__half2float(static_cast<const __half*>(base)[idx]), -f16_exp(amax[f]));
+}
+
+// Where the forward step writes slot t: the strips themselves (f32, bf16) or
+// the f16 staging ring slot t & 1 (floats).
+__device__ __forceinline__ void* strip_save_ptr(const StepArgs& p, const ShotDesc& d) {
+    if (p.strip_prec == kStripF16) return d.stage + (size_t)(p.t & 1) * p.strip_slot;
+    return static_cast<char*>(d.strips) + (size_t)p.t * slot_bytes(p);
+}
+
+__device__ __forceinline__ void strip_put(const StepArgs& p, void* base, int idx, float v) {
+    if (p.strip_prec == kStripBF16) static_cast<__nv_bfloat16*>(base)[idx] = __float2bfloat16_rn(v);
+    else static_cast<float*>(base)[idx] = v;
+}
+
+// Fold per-thread maxima of |v| into a slot's field maxima (f16 strips):
+// one atomic per warp and field.
+template <int NF>
+__device__ __forceinline__ void amax_commit(unsigned* amax, int f0, const float (&m)[NF]) {
+#pragma unroll
+    for (int q = 0; q < NF; ++q) {
+        float v = m[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0 && v > 0.f) atomicMax(amax + f0 + q, __float_as_uint(v));
+    }
 }
 
 // Tile flags, uniform per CTA.
@@ -271,7 +331,7 @@ __device__ __forceinline__ TileFlags tile_flags(const StepArgs& p, const ShotVie
     const bool src_in_s = sv.sx >= s_i0 && sv.sx < s_i1 && sv.sz >= s_j0 && sv.sz < s_j1;
     if (MODE == kRec) {
         f.border = !(x0 >= L && x0 + G::TX <= X - L && z0 >= L && z0 + G::TZ <= Z - L);
-        f.ring = sv.strip_u != nullptr &&
+        f.ring = sv.strips &&
                  rect_meets_ring(p.ring, x0 - G::SHX - N, x0 + G::TX + G::SHX + N, z0 - G::HU, z0 + G::TZ + G::HU);
         f.src = p.src_recon && src_in_s;
         return f;
@@ -281,7 +341,7 @@ __device__ __forceinline__ TileFlags tile_flags(const StepArgs& p, const ShotVie
     f.pz = s_j0 < L || s_j1 - 1 >= Z - L;
     f.border = !(s_i0 >= N && s_i1 <= X - N && s_j0 >= N && s_j1 <= Z - N);
     if (MODE == kFwd) {
-        f.ring = sv.strip_save != nullptr && rect_meets_ring(p.ring, x0, x0 + G::TX, z0, z0 + G::TZ);
+        f.ring = p.save && sv.strips && rect_meets_ring(p.ring, x0, x0 + G::TX, z0, z0 + G::TZ);
         f.src = (sv.src_type == 0 && src_in_s) ||
                 (sv.src_type == 1 && sv.sx >= x0 && sv.sx < x0 + G::TX && sv.sz >= z0 && sv.sz < z0 + G::TZ);
     }
@@ -345,10 +405,13 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
     if (MODE == kRec && f.ring) {
         __syncthreads();
         // reconstruction: the ring comes from the saved strips (read_wavefiled1, PS:1344-1376)
+        const ShotDesc& d = p.shots[blockIdx.y];
+        const void* su = strip_slot_ptr(p, d, p.slot_u);
+        const unsigned* am = d.amax ? d.amax + (size_t)p.slot_u * kStripFields : nullptr;
         for_ring(p.ring, ux_i0, ux_i0 + G::UR, ux_j0, ux_j0 + UC, [&](int i, int j, int ri) {
             const int o = (i - ux_i0) * UC + (j - ux_j0);
-            sUx[o] = sv.strip_u[kSUx * R + ri];
-            sUz[o] = sv.strip_u[kSUz * R + ri];
+            sUx[o] = strip_get(p, su, am, kSUx, kSUx * R + ri);
+            sUz[o] = strip_get(p, su, am, kSUz, kSUz * R + ri);
         });
     }
     __syncthreads();
@@ -447,39 +510,45 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
     }
     if (f.ring) {
         __syncthreads();
+        const ShotDesc& d = p.shots[blockIdx.y];
         if (MODE == kRec) {
             // read_wavefiled2 (PS:1377-1424): theta, omega and the Q fields of the ring
+            const void* ss = strip_slot_ptr(p, d, p.slot_s);
+            const unsigned* am = d.amax ? d.amax + (size_t)p.slot_s * kStripFields : nullptr;
             for_ring(p.ring, x0 - SHX, x0 + TX + SHX, z0 - HS, z0 + TZ + HS, [&](int i, int j, int ri) {
                 const int r = i - x0, c = j - z0;
                 const bool rin = r >= 0 && r < TX, cin = c >= 0 && c < TZ;
                 if (rin || cin) {
                     const int o = (r + SHX) * SC + (c + HS);
-                    sTh[o] = sv.strip_s[kSTh * R + ri];
-                    sOm[o] = sv.strip_s[kSOm * R + ri];
+                    sTh[o] = strip_get(p, ss, am, kSTh, kSTh * R + ri);
+                    sOm[o] = strip_get(p, ss, am, kSOm, kSOm * R + ri);
                 }
                 if (cin) {
-                    sQxz[(r + SHX) * TZ + c] = sv.strip_s[kSQxz * R + ri];
-                    sQzz[(r + SHX) * TZ + c] = sv.strip_s[kSQzz * R + ri];
+                    sQxz[(r + SHX) * TZ + c] = strip_get(p, ss, am, kSQxz, kSQxz * R + ri);
+                    sQzz[(r + SHX) * TZ + c] = strip_get(p, ss, am, kSQzz, kSQzz * R + ri);
                 }
                 if (rin) {
-                    sQxx[r * SC + (c + HS)] = sv.strip_s[kSQxx * R + ri];
-                    sQzx[r * SC + (c + HS)] = sv.strip_s[kSQzx * R + ri];
+                    sQxx[r * SC + (c + HS)] = strip_get(p, ss, am, kSQxx, kSQxx * R + ri);
+                    sQzx[r * SC + (c + HS)] = strip_get(p, ss, am, kSQzx, kSQzx * R + ri);
                 }
             });
         }
         if (MODE == kFwd) {
             // save_wavefiled (PS:1230-1287): the S fields of the tile's ring cells
-            float* s = sv.strip_save;
+            void* s = strip_save_ptr(p, d);
+            float m[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             for_ring(p.ring, x0, x0 + TX, z0, z0 + TZ, [&](int i, int j, int ri) {
                 const int r = i - x0, c = j - z0;
                 const int o = (r + SHX) * SC + (c + HS);
-                s[kSTh * R + ri] = sTh[o];
-                s[kSOm * R + ri] = sOm[o];
-                s[kSQzx * R + ri] = sQzx[r * SC + (c + HS)];
-                s[kSQzz * R + ri] = sQzz[(r + SHX) * TZ + c];
-                s[kSQxx * R + ri] = sQxx[r * SC + (c + HS)];
-                s[kSQxz * R + ri] = sQxz[(r + SHX) * TZ + c];
+                const float v[6] = {sTh[o], sOm[o], sQzx[r * SC + (c + HS)], sQzz[(r + SHX) * TZ + c],
+                                    sQxx[r * SC + (c + HS)], sQxz[(r + SHX) * TZ + c]};
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    strip_put(p, s, (kSTh + q) * R + ri, v[q]);
+                    m[q] = fmaxf(m[q], fabsf(v[q]));
+                }
             });
+            if (p.strip_prec == kStripF16) amax_commit<6>(d.amax + (size_t)p.t * kStripFields, kSTh, m);
         }
     }
     __syncthreads();
@@ -581,18 +650,45 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
                                 add2(hi2(acc), fma2(hi2(a1), hi2(b1), mul2(hi2(a2), hi2(b2)))));
                 };
                 const float4 o0 = ld4(acc0), o1 = ld4(acc1), o2 = ld4(acc2);
-                float4 npp = corr(o0, sx, rpx, sz, rpz);
-                float4 nil = corr(o2, sx, sx, sz, sz);
-                float4 nps = corr(o1, sx, rsx, sz, rsz);
-                if (f.border) {
+                if (!p.comp_image) {
+                    float4 npp = corr(o0, sx, rpx, sz, rpz);
+                    float4 nil = corr(o2, sx, sx, sz, sz);
+                    float4 nps = corr(o1, sx, rsx, sz, rsz);
+                    if (f.border) {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (!(live & (1u << k))) {
-                            set_comp(npp, k, comp(o0, k)); set_comp(nps, k, comp(o1, k)); set_comp(nil, k, comp(o2, k));
+                        for (int k = 0; k < 4; ++k) {
+                            if (!(live & (1u << k))) {
+                                set_comp(npp, k, comp(o0, k)); set_comp(nps, k, comp(o1, k)); set_comp(nil, k, comp(o2, k));
+                            }
                         }
                     }
+                    st4(acc0, npp); st4(acc1, nps); st4(acc2, nil);
+                } else {
+                    // compensated sums (Kahan, CACM 8(1), 1965): acc + c carries the
+                    // sum to about twice float precision; c holds minus the
+                    // low-order part lost by the last addition
+                    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float4 tpp = corr(zero, sx, rpx, sz, rpz), tps = corr(zero, sx, rsx, sz, rsz);
+                    const float4 til = corr(zero, sx, sx, sz, sz);
+                    float* cp[3] = {p.comp[0] + off + g, p.comp[1] + off + g, p.comp[2] + off + g};
+                    const float4 term[3] = {tpp, tps, til}, old[3] = {o0, o1, o2};
+                    float* accp[3] = {acc0, acc1, acc2};
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const float4 cq = ld4(cp[q]);
+                        float4 na = old[q], nc = cq;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (f.border && !(live & (1u << k))) continue;
+                            const float y = __fsub_rn(comp(term[q], k), comp(cq, k));
+                            const float t = __fadd_rn(comp(old[q], k), y);
+                            set_comp(nc, k, __fsub_rn(__fsub_rn(t, comp(old[q], k)), y));
+                            set_comp(na, k, t);
+                        }
+                        st4(accp[q], na);
+                        st4(cp[q], nc);
+                    }
                 }
-                st4(acc0, npp); st4(acc1, nps); st4(acc2, nil);
             }
             st4(p.past[0] + off + g, vpx); st4(p.past[1] + off + g, vpz);
             st4(p.past[2] + off + g, vsx); st4(p.past[3] + off + g, vsz);
@@ -609,12 +705,35 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const ShotView& sv,
     if (MODE == kFwd && f.ring) {
         // save_wavefiled (PS:1230-1287): the new displacement of the tile's ring cells
         __syncthreads();
-        float* s = sv.strip_save;
+        const ShotDesc& d = p.shots[blockIdx.y];
+        void* s = strip_save_ptr(p, d);
+        float m[2] = {0.f, 0.f};
         for_ring(p.ring, x0, x0 + TX, z0, z0 + TZ, [&](int i, int j, int ri) {
             const int o = (i - x0) * TZ + (j - z0);
-            s[kSUx * R + ri] = sUx[o];
-            s[kSUz * R + ri] = sUz[o];
+            const float ux = sUx[o], uz = sUz[o];
+            strip_put(p, s, kSUx * R + ri, ux);
+            strip_put(p, s, kSUz * R + ri, uz);
+            m[0] = fmaxf(m[0], fabsf(ux));
+            m[1] = fmaxf(m[1], fabsf(uz));
         });
+        if (p.strip_prec == kStripF16) {
+            amax_commit<2>(d.amax + (size_t)p.t * kStripFields, kSUx, m);
+            if (p.t > 0) {
+                // slot t-1 is complete (its maxima with it): convert this tile's
+                // cells of it from the staging ring to scaled halves
+                const float* src = d.stage + (size_t)((p.t - 1) & 1) * p.strip_slot;
+                __half* dst = reinterpret_cast<__half*>(static_cast<char*>(d.strips) + (size_t)(p.t - 1) * slot_bytes(p));
+                const unsigned* am = d.amax + (size_t)(p.t - 1) * kStripFields;
+                int k[kStripFields];
+#pragma unroll
+                for (int q = 0; q < kStripFields; ++q) k[q] = f16_exp(am[q]);
+                for_ring(p.ring, x0, x0 + TX, z0, z0 + TZ, [&](int, int, int ri) {
+#pragma unroll
+                    for (int q = 0; q < kStripFields; ++q)
+                        dst[q * R + ri] = __float2half_rn(scale2(src[q * R + ri], k[q]));
+                });
+            }
+        }
     }
 }
 

@@ -3,6 +3,8 @@
 // transposes, field packing).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fd_step.cuh"
 #include "ouc_internal.h"
 
@@ -77,6 +79,13 @@ void launch_image_only(const StepArgs& a, int nshots, cudaStream_t s) {
 // nx x nz and added into the FP64 stack.
 __device__ __forceinline__ float img_at(const float* num, const float* den, ptrdiff_t g) { return num[g] / den[g]; }
 
+// The same from compensated sums: value = acc - c, the quotient formed in
+// double and rounded once.
+__device__ __forceinline__ float img_at_comp(const float* num, const float* cn, const float* den, const float* cd,
+                                             ptrdiff_t g) {
+    return (float)(((double)num[g] - (double)cn[g]) / ((double)den[g] - (double)cd[g]));
+}
+
 __global__ void k_finalize(const FinalizeArgs f) {
     const int nx = f.X - 2 * f.L, nz = f.Z - 2 * f.L;
     const int ii = blockIdx.y;
@@ -94,10 +103,18 @@ __global__ void k_finalize(const FinalizeArgs f) {
                 const float* den = f.acc[2];
                 const ptrdiff_t P = f.pitch;
                 const float c = 1 / f.dh / f.dh;
-                lpp = c * (img_at(npp, den, g + P) + img_at(npp, den, g - P) - 2 * img_at(npp, den, g) +
-                           img_at(npp, den, g + 1) + img_at(npp, den, g - 1) - 2 * img_at(npp, den, g));
-                lps = c * (img_at(nps, den, g + P) + img_at(nps, den, g - P) - 2 * img_at(nps, den, g) +
-                           img_at(nps, den, g + 1) + img_at(nps, den, g - 1) - 2 * img_at(nps, den, g));
+                if (!f.comp[0]) {
+                    lpp = c * (img_at(npp, den, g + P) + img_at(npp, den, g - P) - 2 * img_at(npp, den, g) +
+                               img_at(npp, den, g + 1) + img_at(npp, den, g - 1) - 2 * img_at(npp, den, g));
+                    lps = c * (img_at(nps, den, g + P) + img_at(nps, den, g - P) - 2 * img_at(nps, den, g) +
+                               img_at(nps, den, g + 1) + img_at(nps, den, g - 1) - 2 * img_at(nps, den, g));
+                } else {
+                    const float *cpp = f.comp[0], *cps = f.comp[1], *cd = f.comp[2];
+                    auto ip = [&](ptrdiff_t q) { return img_at_comp(npp, cpp, den, cd, q); };
+                    auto is = [&](ptrdiff_t q) { return img_at_comp(nps, cps, den, cd, q); };
+                    lpp = c * (ip(g + P) + ip(g - P) - 2 * ip(g) + ip(g + 1) + ip(g - 1) - 2 * ip(g));
+                    lps = c * (is(g + P) + is(g - P) - 2 * is(g) + is(g + 1) + is(g - 1) - 2 * is(g));
+                }
             }
             if (f.img) {
                 f.img[((size_t)b * 2 + 0) * nx * nz + o] = lpp;
@@ -105,7 +122,7 @@ __global__ void k_finalize(const FinalizeArgs f) {
             }
             spp += (double)lpp;
             sps += (double)lps;
-            sil += (double)f.acc[2][g];
+            sil += f.illum_scale * (f.comp[2] ? (double)f.acc[2][g] - (double)f.comp[2][g] : (double)f.acc[2][g]);
         }
         if (f.stack[0]) {
             f.stack[0][o] += spp;
@@ -113,6 +130,140 @@ __global__ void k_finalize(const FinalizeArgs f) {
             f.stack[2][o] += sil;
         }
     }
+}
+
+// Conversion of one f16 strip slot from the staging ring once its field
+// maxima are complete (the forward step converts slot t-1 itself; this
+// converts the last slot).  blockIdx.y = shot.
+__global__ void k_strip_pack(const ShotDesc* shots, int slot, int ring, size_t strip_slot) {
+    const ShotDesc& d = shots[blockIdx.y];
+    const float* src = d.stage + (size_t)(slot & 1) * strip_slot;
+    __half* dst = reinterpret_cast<__half*>(d.strips) + (size_t)slot * strip_slot;
+    const unsigned* am = d.amax + (size_t)slot * kStripFields;
+    for (size_t e = threadIdx.x + (size_t)blockIdx.x * blockDim.x; e < strip_slot; e += (size_t)blockDim.x * gridDim.x) {
+        const int f = (int)(e / ring);
+        dst[e] = __float2half_rn(scale2(src[e], f16_exp(am[f])));
+    }
+}
+
+void launch_strip_pack(const ShotDesc* shots, int nshots, int slot, int ring, size_t strip_slot, cudaStream_t s) {
+    const int blocks = (int)std::min<size_t>((strip_slot + 255) / 256, 1184);
+    k_strip_pack<<<dim3(blocks, nshots), 256, 0, s>>>(shots, slot, ring, strip_slot);
+}
+
+// ---- source-wavefield snapshots ---------------------------------------------
+
+__device__ __forceinline__ size_t snap_index(const SnapArgs& a, int b, int comp, int ii, int jj) {
+    return (size_t)b * a.shot_elems + ((size_t)a.slot * 2 + comp) * a.nx * a.nz + (size_t)ii * a.nz + jj;
+}
+
+// Largest |Px|, |Pz| of each shot's interior (f16 snapshots): block maxima,
+// then one atomic per block and component.  grid (z blocks, nx, shots).
+__global__ void k_snap_amax(const SnapArgs a) {
+    const int ii = blockIdx.y, b = blockIdx.z;
+    const size_t off = (size_t)b * a.shot_stride;
+    float m0 = 0.f, m1 = 0.f;
+    for (int jj = threadIdx.x + blockIdx.x * blockDim.x; jj < a.nz; jj += blockDim.x * gridDim.x) {
+        const ptrdiff_t g = (ptrdiff_t)(ii + a.L) * a.pitch + (jj + a.L) + off;
+        m0 = fmaxf(m0, fabsf(a.px[g]));
+        m1 = fmaxf(m1, fabsf(a.pz[g]));
+    }
+    __shared__ float red[2][32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m0 = fmaxf(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+        m1 = fmaxf(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    }
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = m0; red[1][w] = m1; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        float m = 0.f;
+        for (int q = 0; q < nw; ++q) m = fmaxf(m, red[threadIdx.x][q]);
+        if (m > 0.f) atomicMax(a.amax + ((size_t)b * a.nslots + a.slot) * 2 + threadIdx.x, __float_as_uint(m));
+    }
+}
+
+// Store the interior Px, Pz as snapshot `slot` in the snapshot type.
+__global__ void k_snap_store(const SnapArgs a) {
+    const int ii = blockIdx.y, b = blockIdx.z;
+    const size_t off = (size_t)b * a.shot_stride;
+    int k0 = 0, k1 = 0;
+    if (a.prec == kStripF16) {
+        const unsigned* am = a.amax + ((size_t)b * a.nslots + a.slot) * 2;
+        k0 = f16_exp(am[0]);
+        k1 = f16_exp(am[1]);
+    }
+    for (int jj = threadIdx.x + blockIdx.x * blockDim.x; jj < a.nz; jj += blockDim.x * gridDim.x) {
+        const ptrdiff_t g = (ptrdiff_t)(ii + a.L) * a.pitch + (jj + a.L) + off;
+        const float v0 = a.px[g], v1 = a.pz[g];
+        const size_t e0 = snap_index(a, b, 0, ii, jj), e1 = snap_index(a, b, 1, ii, jj);
+        if (a.prec == kStripF32) {
+            static_cast<float*>(a.snaps)[e0] = v0;
+            static_cast<float*>(a.snaps)[e1] = v1;
+        } else if (a.prec == kStripBF16) {
+            static_cast<__nv_bfloat16*>(a.snaps)[e0] = __float2bfloat16_rn(v0);
+            static_cast<__nv_bfloat16*>(a.snaps)[e1] = __float2bfloat16_rn(v1);
+        } else {
+            static_cast<__half*>(a.snaps)[e0] = __float2half_rn(scale2(v0, k0));
+            static_cast<__half*>(a.snaps)[e1] = __float2half_rn(scale2(v1, k1));
+        }
+    }
+}
+
+void launch_snap_store(const SnapArgs& a, int nshots, cudaStream_t s) {
+    const dim3 grid((a.nz + 255) / 256, a.nx, nshots);
+    if (a.prec == kStripF16) k_snap_amax<<<grid, 256, 0, s>>>(a);
+    k_snap_store<<<grid, 256, 0, s>>>(a);
+}
+
+__device__ __forceinline__ float snap_get(const SnapArgs& a, size_t e, int k) {
+    if (a.prec == kStripF32) return static_cast<const float*>(a.snaps)[e];
+    if (a.prec == kStripBF16) return __bfloat162float(static_cast<const __nv_bfloat16*>(a.snaps)[e]);
+    return scale2(__half2float(static_cast<const __half*>(a.snaps)[e]), -k);
+}
+
+__device__ __forceinline__ void kahan_add(float* acc, float* c, float term) {
+    const float y = __fsub_rn(term, *c);
+    const float t = __fadd_rn(*acc, y);
+    *c = __fsub_rn(__fsub_rn(t, *acc), y);
+    *acc = t;
+}
+
+// Zero-lag imaging at a snapshot level: the stored source P against the
+// receiver wavefield after its back-step, with the rounding of corr_v
+// (acc + fma(p, q, u v), PS:1434-1436).  grid (z blocks, nx, shots).
+__global__ void k_image_snap(const SnapArgs a) {
+    const int ii = blockIdx.y, b = blockIdx.z;
+    const size_t off = (size_t)b * a.shot_stride;
+    int k0 = 0, k1 = 0;
+    if (a.prec == kStripF16) {
+        const unsigned* am = a.amax + ((size_t)b * a.nslots + a.slot) * 2;
+        k0 = f16_exp(am[0]);
+        k1 = f16_exp(am[1]);
+    }
+    for (int jj = threadIdx.x + blockIdx.x * blockDim.x; jj < a.nz; jj += blockDim.x * gridDim.x) {
+        const ptrdiff_t g = (ptrdiff_t)(ii + a.L) * a.pitch + (jj + a.L) + off;
+        const float sx = snap_get(a, snap_index(a, b, 0, ii, jj), k0);
+        const float sz = snap_get(a, snap_index(a, b, 1, ii, jj), k1);
+        const float rpx = a.rcv[0][g], rpz = a.rcv[1][g], rsx = a.rcv[2][g], rsz = a.rcv[3][g];
+        const float tpp = __fmaf_rn(sx, rpx, __fmul_rn(sz, rpz));
+        const float tps = __fmaf_rn(sx, rsx, __fmul_rn(sz, rsz));
+        const float til = __fmaf_rn(sx, sx, __fmul_rn(sz, sz));
+        if (!a.comp_image) {
+            a.acc[0][g] = __fadd_rn(a.acc[0][g], tpp);
+            a.acc[1][g] = __fadd_rn(a.acc[1][g], tps);
+            a.acc[2][g] = __fadd_rn(a.acc[2][g], til);
+        } else {
+            kahan_add(a.acc[0] + g, a.comp[0] + g, tpp);
+            kahan_add(a.acc[1] + g, a.comp[1] + g, tps);
+            kahan_add(a.acc[2] + g, a.comp[2] + g, til);
+        }
+    }
+}
+
+void launch_image_snap(const SnapArgs& a, int nshots, cudaStream_t s) {
+    k_image_snap<<<dim3((a.nz + 255) / 256, a.nx, nshots), 256, 0, s>>>(a);
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {

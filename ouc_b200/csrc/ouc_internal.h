@@ -61,13 +61,28 @@ struct Ring {
 // Ux, Uz, theta, omega, Qzx, Qzz, Qxx, Qxz.
 enum StripField : int { kSUx = 0, kSUz, kSTh, kSOm, kSQzx, kSQzz, kSQxx, kSQxz, kStripFields };
 
+// Storage of the boundary strips (ouc_config.strip_precision).
+//   kStripF32:  float, as computed;
+//   kStripF16:  IEEE half of v * 2^k, one power-of-two scale k per slot and
+//               field, chosen from that slot's largest |v| so that it maps
+//               into [2^14, 2^15); the forward step writes float values to a
+//               two-slot staging ring and reduces their maxima, and the next
+//               step (or k_strip_pack after the last one) converts the slot
+//               once its maxima are complete;
+//   kStripBF16: bfloat16 of v (float's exponent range: no scale).
+enum StripPrec : int { kStripF32 = 0, kStripF16 = 1, kStripBF16 = 2 };
+
+__host__ __device__ constexpr int strip_elem_bytes(int prec) { return prec == kStripF32 ? 4 : 2; }
+
 // Per-shot constants of a batch (uploaded once per batch).
 struct ShotDesc {
     int sx, sz, rz, src_type;      // padded coordinates
     const float* wavelet;          // nt samples
     float* gather_x;               // time-major gathers [nt][X]
     float* gather_z;
-    float* strips;                 // [slot][8 fields][ring] or null
+    void* strips;                  // [slot][8 fields][ring] of the strip element type, or null
+    float* stage;                  // kStripF16: staging ring [2][8 fields][ring] floats
+    unsigned* amax;                // kStripF16: [slot][8 fields] bits of the largest |v| (float)
 };
 
 struct StepArgs {
@@ -78,6 +93,8 @@ struct StepArgs {
     int record, save;                 // kFwd: write gathers / boundary strips this step
     int src_recon;                    // kRec: add the source term at (sx, sz) outside the ring
     int img_past;                     // kRec: correlate with level t+2 (reference alignment)
+    int strip_prec;                   // StripPrec of the strips
+    int comp_image;                   // kRec: compensated (Kahan) imaging sums, comp[] below
     float a[6];                       // stencil weights a_1..a_N
     float dx, dz, dt, dt2;
     float rdx, rdz;                   // RN(1/dx), RN(1/dz)
@@ -94,6 +111,7 @@ struct StepArgs {
     // kRec imaging
     const float* rcv[4];              // receiver Px Pz Sx Sz after this back-step
     float* acc[3];                    // PP, PS, illumination accumulators
+    float* comp[3];                   // their compensation terms (comp_image)
     // model (shared by the batch)
     const float* vp2;
     const float* vs2;
@@ -111,8 +129,34 @@ struct FinalizeArgs {
     size_t shot_stride;    // between shots' accumulators (floats)
     float dh;
     const float* acc[3];   // shot 0
+    const float* comp[3];  // compensation terms of the accumulators, or null (plain sums)
     float* img;            // [shot][2][nx][nz] dense, or null
     double* stack[3];      // nx*nz dense FP64: PP, PS, illumination (or null)
+    double illum_scale;    // illumination into the stack x this (imaged levels: every K-th)
+};
+
+// Source-wavefield snapshots (ouc_config.snapshot_every = K >= 1): the
+// source P displacement (Px, Pz) on the interior at every K-th imaging level,
+// stored as [shot][slot][2][nx][nz] elements of the strip type (StripPrec),
+// f16 scaled by 2^k per slot and component (k from that snapshot's largest
+// |v|, as for the strips).  The backward pass images those levels only.
+struct SnapArgs {
+    int X, Z, pitch, L, nx, nz;
+    size_t shot_stride;      // state floats between shots
+    int prec;                // StripPrec of the snapshots
+    int slot;
+    size_t shot_elems;       // snapshot elements per shot (all slots)
+    void* snaps;             // shot 0, slot 0
+    unsigned* amax;          // f16: [shot][slot][2] bits of the largest |v|
+    int nslots;
+    // pack: the source P level to store (shot 0, pitched)
+    const float* px;
+    const float* pz;
+    // imaging: receiver fields after the back-step, accumulators (shot 0)
+    const float* rcv[4];
+    float* acc[3];
+    float* comp[3];
+    int comp_image;
 };
 
 // Host-side launchers (kernels.cu)
@@ -124,5 +168,8 @@ void launch_mute(float* gx, float* gz, int X, int nt, int sx, int sz, int rz, in
                  cudaStream_t s);
 void launch_transpose(const float* in, float* out, int rows, int cols, cudaStream_t s);
 void launch_pack_fields(const float* const* f, int nf, int X, int Z, int pitch, float* out, cudaStream_t s);
+void launch_strip_pack(const ShotDesc* shots, int nshots, int slot, int ring, size_t strip_slot, cudaStream_t s);
+void launch_snap_store(const SnapArgs& a, int nshots, cudaStream_t s);
+void launch_image_snap(const SnapArgs& a, int nshots, cudaStream_t s);
 
 }  // namespace ouc

@@ -78,3 +78,7 @@ def test_create_rejects_bad_configs_without_touching_the_device():
     assert e.value.code == 1
     with pytest.raises(ValueError):
         o.Context(o.Config(**base), vp[:10], vs)
+    for bad_cfg in ({"strip_precision": 3}, {"compensated_image": 2}):
+        with pytest.raises(o.OucError) as e:
+            o.Context(o.Config(**base, **bad_cfg), vp, vs)
+        assert e.value.code == 1
