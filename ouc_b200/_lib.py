@@ -67,6 +67,18 @@ SIGNATURES = {
     "ouc_step_reconstruct": (C.c_int, [_vp, C.c_int]),
     "ouc_image_finalize": (C.c_int, [_vp, _fp, _fp]),
     "ouc_step_fields": (C.c_int, [_vp, C.c_int, _fp]),
+    # include/ouc_corrector.h
+    "ouc_cnn_nparams": (C.c_int, []),
+    "ouc_cnn_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "ouc_cnn_destroy": (C.c_int, [_vp]),
+    "ouc_cnn_set_params": (C.c_int, [_vp, _fp]),
+    "ouc_cnn_get_params": (C.c_int, [_vp, _fp]),
+    "ouc_cnn_forward_dev": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "ouc_cnn_backward_dev": (C.c_int, [_vp, _vp, _vp]),
+    "ouc_cnn_zero_grad": (C.c_int, [_vp, _vp]),
+    "ouc_cnn_get_grads": (C.c_int, [_vp, _fp]),
+    "ouc_cnn_adam_step": (C.c_int, [_vp, C.c_float, C.c_float, C.c_float, C.c_float, _vp]),
+    "ouc_cnn_error": (C.c_int, [_vp]),
 }
 
 _lib = None
