@@ -1,7 +1,7 @@
 """CPU restatement of the learned corrector's network (test infrastructure).
 
 Checks the tensor-core kernels of ouc_b200/csrc/corrector.cu: the same
-four-layer 5x5 CNN (5 -> 32 -> 32 -> 32 -> 8 channels, ReLU between, "same"
+four-layer 5x5 CNN (10 -> 32 -> 32 -> 32 -> 8 channels, ReLU between, "same"
 zero padding), computed in float64 with the operands rounded to bfloat16 at
 the points where the GPU path rounds them (network input, weights, hidden
 activations, output and hidden-layer gradients), so that the two differ only
@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 
-DIMS = [(5, 32), (32, 32), (32, 32), (32, 8)]
+DIMS = [(10, 32), (32, 32), (32, 32), (32, 8)]
 TAPS = 25
 
 

@@ -79,6 +79,13 @@ SIGNATURES = {
     "ouc_cnn_get_grads": (C.c_int, [_vp, _fp]),
     "ouc_cnn_adam_step": (C.c_int, [_vp, C.c_float, C.c_float, C.c_float, C.c_float, _vp]),
     "ouc_cnn_error": (C.c_int, [_vp]),
+    "ouc_cnn_train": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.c_int, C.c_int, C.c_float, C.c_uint, _fp, _vp]),
+    "ouc_coarse_wavelet": (C.c_int, [_fp, C.c_int, _fp]),
+    "ouc_forward_learned": (C.c_int, [_vp, _vp, C.POINTER(ouc_shot), _fp, C.c_int, _fp, _fp]),
+    "ouc_forward_restricted": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, C.c_int, _fp, _fp]),
+    "ouc_learned_pairs": (C.c_int, [_vp, _vp, _vp, C.POINTER(ouc_shot), _fp, C.c_int, C.c_float, C.c_uint, C.c_int,
+                                    _vp, _vp, C.POINTER(C.c_int)]),
 }
 
 _lib = None

@@ -12,7 +12,7 @@ import numpy as np
 from . import _lib
 from ._lib import lib
 
-N_IN, WIDTH, N_OUT = 5, 32, 8
+N_IN, WIDTH, N_OUT = 10, 32, 8
 
 
 def _fp(a):

@@ -20,6 +20,7 @@
 
 #include "../../include/ouc.h"
 #include "ouc_internal.h"
+#include "ctx.h"
 
 using namespace ouc;
 
@@ -42,77 +43,11 @@ const double kWeights[7][6] = {
     {1.2213364, -9.6931458e-2, 1.7447662e-2, -2.9672895e-3, 3.5900540e-4, -2.1847812e-5},
 };
 
-constexpr int kFieldsPerSide = 24;                    // now 4, past 4, F old 4, F new 4, O 8
-constexpr int kFieldsPerShot = 2 * kFieldsPerSide + 6;   // source side, receiver side, accumulators + compensation
-
-// Field pointers of one wavefield (shot 0 of the batch).
-struct Side {
-    float* now[4];
-    float* past[4];
-    float* fo[4];
-    float* fn[4];
-    float* o[8];
-    void swap_levels() { for (int k = 0; k < 4; ++k) std::swap(now[k], past[k]); }
-    void swap_memory() { for (int k = 0; k < 4; ++k) std::swap(fo[k], fn[k]); }
-};
-
 }  // namespace
 
-struct ouc_ctx {
-    ouc_config cfg;
-    int X = 0, Z = 0, L = 0, N = 0, nx = 0, nz = 0, nt = 0;
-    int Xc = 0, Zc = 0, pitch = 0;
-    int batch = 1;               // shots per launch
-    size_t fstride = 0;          // floats per field allocation
-    size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
-    int tiles_x = 0, tiles_z = 0;
-    int rec_tx0 = 0, rec_tz0 = 0, rec_tiles_x = 0, rec_tiles_z = 0;
-    float a[6] = {0, 0, 0, 0, 0, 0};
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int device = 0;
-    std::string err;
-    ouc_timing timing{};
-    Ring ring{};
-    std::vector<float> vp_host;  // padded Vp (for the mute's velocity)
 
-    // device memory
-    float* model = nullptr;      // 4 fields: vp2 vs2 ax az
-    float* state = nullptr;      // batch shot blocks
-    float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
-    Side src{}, rcv{};
-    float* acc[3] = {nullptr, nullptr, nullptr};
-    float* comp[3] = {nullptr, nullptr, nullptr};   // compensation terms of acc (compensated_image)
-    float* gathers = nullptr;    // [batch][2][nt][X], time-major
-    float* staging = nullptr;    // max(nt*X, 4*X*Z) floats for transposes / packing
-    float* d_wavelet = nullptr;
-    float* d_img = nullptr;      // [batch][2][nx][nz]
-    double* d_stack[3] = {nullptr, nullptr, nullptr};
-    void* strips = nullptr;      // [batch][nt][8][R] of the strip element type
-    float* stage = nullptr;      // f16 strips: staging rings [batch][2][8][R]
-    unsigned* amax = nullptr;    // f16 strips: per-slot field maxima [batch][nt][8]
-    // snapshot form (cfg.snapshot_every = K >= 1)
-    void* snaps = nullptr;       // [batch][nslots][2][nx][nz] of the strip element type
-    unsigned* snap_amax = nullptr;   // f16: [batch][nslots][2]
-    int nslots = 0;
-    std::vector<int> snap_fwd;   // forward step -> snapshot slot of its new level, or -1
-    std::vector<int> snap_bwd;   // backward step -> slot imaged there, or -1
-    size_t strip_slot = 0;       // floats per slot
-    ShotDesc* d_desc = nullptr;  // [batch]
-    size_t bytes = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-
-    // step-level interface: one shot (slot 0) advanced one launch per call
-    enum { kIdle, kForward, kReceiver, kReconstruct, kFinalize } step_phase = kIdle;
-    int step_t = 0;              // the time the next step call must name
-    ouc_shot step_shot{};
-    StepArgs step_fwd{}, step_rcv{}, step_rec{};
-
-    float* field(float* base, size_t k) const { return base + k * fstride + (size_t)kGX * pitch + kZOFF; }
-    float* gather(int b, int comp) const { return gathers + ((size_t)b * 2 + comp) * (size_t)nt * X; }
-};
-
-namespace {
+namespace ouc {
+namespace host {
 
 int fail(ouc_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -316,7 +251,7 @@ int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t) {
 
 // Forward time loop (PS:2258-2292) of n shots.  Records into the time-major
 // gathers when `record`, saves the boundary ring of every step when `save`.
-int run_forward(ouc_ctx* ctx, int n, bool record, bool save, bool snaps = false) {
+int run_forward(ouc_ctx* ctx, int n, bool record, bool save, bool snaps) {
     Side s = ctx->src;
     int rc = zero_side(ctx, n, 0, false);
     if (rc) return rc;
@@ -491,7 +426,10 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace ouc
+
+using namespace ouc::host;
 
 extern "C" {
 
@@ -703,6 +641,7 @@ int ouc_destroy(ouc_ctx* ctx) {
     for (auto* p : ctx->d_stack) cudaFree(p);
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
+    cudaFree(ctx->l_in); cudaFree(ctx->l_out); cudaFree(ctx->l_truth); cudaFree(ctx->l_scale); cudaFree(ctx->l_tmp);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

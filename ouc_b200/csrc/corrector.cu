@@ -25,10 +25,12 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <new>
+#include <random>
 #include <vector>
 
 #include "../../include/ouc.h"
@@ -415,6 +417,27 @@ __global__ void k_adam(int n, float* p, const float* g, float* m, float* v, floa
     }
 }
 
+// Masked mean squared error of n images [n][H][W][8] against targets:
+// g = 2 (y - t) / count on the rectangle [i0, i1) x [j0, j1) of every image
+// and 0 elsewhere; loss += sum (y - t)^2 / count.
+__global__ void k_mse(int n, int H, int W, int i0, int i1, int j0, int j1, float inv_count, const float* y,
+                      const float* t, float* g, double* loss) {
+    double acc = 0.0;
+    const size_t P = (size_t)n * H * W;
+    for (size_t p = threadIdx.x + (size_t)blockIdx.x * blockDim.x; p < P; p += (size_t)blockDim.x * gridDim.x) {
+        const int j = (int)(p % W), i = (int)((p / W) % H);
+        const bool in = i >= i0 && i < i1 && j >= j0 && j < j1;
+#pragma unroll
+        for (int c = 0; c < OUC_CNN_OUT; ++c) {
+            const float d = in ? y[p * OUC_CNN_OUT + c] - t[p * OUC_CNN_OUT + c] : 0.f;
+            g[p * OUC_CNN_OUT + c] = 2.f * d * inv_count;
+            acc += (double)d * d;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc * inv_count);
+}
+
 }  // namespace cnn
 }  // namespace ouc
 
@@ -625,6 +648,61 @@ int ouc_cnn_adam_step(ouc_cnn* net, float lr, float beta1, float beta2, float ep
     const float lr_t = (float)(lr * std::sqrt(c2) / c1);
     k_adam<<<64, 256, 0, s>>>(kNParams, net->params, net->grads, net->adam_m, net->adam_v, lr_t, beta1, beta2, eps);
     return repack(net, s);
+}
+
+int ouc_cnn_train(ouc_cnn* net, const float* d_in, const float* d_tgt, int npairs, int H, int W, int i0, int i1, int j0,
+                  int j1, int batch, int epochs, float lr, unsigned seed, float* epoch_loss, void* stream) {
+    if (!net || !d_in || !d_tgt || npairs < 1 || H < 1 || W < 1 || batch < 1 || epochs < 1 || !(lr > 0)) return OUC_EINVAL;
+    if (!(0 <= i0 && i0 < i1 && i1 <= H && 0 <= j0 && j0 < j1 && j1 <= W)) return OUC_EINVAL;
+    cudaSetDevice(net->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    batch = std::min(batch, npairs);
+    const size_t img = (size_t)H * W;
+    float *bin = nullptr, *btg = nullptr, *by = nullptr, *bg = nullptr;
+    double* dloss = nullptr;
+    bool ok = cudaMalloc(&bin, batch * img * OUC_CNN_IN * 4) == cudaSuccess &&
+              cudaMalloc(&btg, batch * img * OUC_CNN_OUT * 4) == cudaSuccess &&
+              cudaMalloc(&by, batch * img * OUC_CNN_OUT * 4) == cudaSuccess &&
+              cudaMalloc(&bg, batch * img * OUC_CNN_OUT * 4) == cudaSuccess &&
+              cudaMalloc(&dloss, sizeof(double)) == cudaSuccess;
+    int rc = ok ? OUC_OK : OUC_ENOMEM;
+    std::vector<int> order(npairs);
+    for (int k = 0; k < npairs; ++k) order[k] = k;
+    std::mt19937 rng(seed);
+    const int nb = (npairs + batch - 1) / batch;
+    for (int e = 0; e < epochs && rc == OUC_OK; ++e) {
+        std::shuffle(order.begin(), order.end(), rng);
+        cudaMemsetAsync(dloss, 0, sizeof(double), s);
+        for (int b = 0; b < nb && rc == OUC_OK; ++b) {
+            const int n = std::min(batch, npairs - b * batch);
+            for (int k = 0; k < n; ++k) {
+                const size_t q = order[b * batch + k];
+                cudaMemcpyAsync(bin + k * img * OUC_CNN_IN, d_in + q * img * OUC_CNN_IN, img * OUC_CNN_IN * 4,
+                                cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(btg + k * img * OUC_CNN_OUT, d_tgt + q * img * OUC_CNN_OUT, img * OUC_CNN_OUT * 4,
+                                cudaMemcpyDeviceToDevice, s);
+            }
+            if ((rc = ouc_cnn_forward_dev(net, n, H, W, bin, by, s))) break;
+            const float inv = 1.f / ((float)n * (i1 - i0) * (j1 - j0) * OUC_CNN_OUT);
+            k_mse<<<592, 256, 0, s>>>(n, H, W, i0, i1, j0, j1, inv, by, btg, bg, dloss);
+            if ((rc = ouc_cnn_zero_grad(net, s)) || (rc = ouc_cnn_backward_dev(net, bg, s))) break;
+            // bias-free network: a zero input gives a zero output
+            for (int l = 0; l < 4; ++l)
+                cudaMemsetAsync(net->grads + p_offset(l) + w_count(l), 0, kL[l].cout * sizeof(float), s);
+            if ((rc = ouc_cnn_adam_step(net, lr, 0.9f, 0.999f, 1e-8f, s))) break;
+        }
+        double l = 0;
+        if (rc == OUC_OK && cudaMemcpyAsync(&l, dloss, sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+            cudaStreamSynchronize(s) == cudaSuccess) {
+            if (epoch_loss) epoch_loss[e] = (float)(l / nb);
+        } else if (rc == OUC_OK) {
+            rc = OUC_ECUDA;
+        }
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(bin); cudaFree(btg); cudaFree(by); cudaFree(bg); cudaFree(dloss);
+    if (rc == OUC_OK && cudaGetLastError() != cudaSuccess) rc = OUC_ECUDA;
+    return rc;
 }
 
 int ouc_cnn_error(ouc_cnn* net) {

@@ -20,7 +20,7 @@ def test_oracle_backward_matches_finite_differences():
     rng = np.random.default_rng(3)
     p = cnn.init_params(seed=5).astype(np.float64)
     p[np.arange(len(p)) % 7 == 0] += 0.01                          # non-zero biases too
-    x = rng.normal(size=(1, 7, 9, 5))
+    x = rng.normal(size=(1, 7, 9, cnn.DIMS[0][0]))
     gout = rng.normal(size=(1, 7, 9, 8))
     net = cnn.Net(p, rounding=False)
     net.forward(x)
@@ -38,5 +38,5 @@ def test_oracle_backward_matches_finite_differences():
 
 
 def test_parameter_count_matches_the_layout():
-    assert cnn.nparams() == 61704
+    assert cnn.nparams() == 65704
     assert len(cnn.init_params()) == cnn.nparams()

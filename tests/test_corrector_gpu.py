@@ -37,7 +37,7 @@ def test_forward_and_gradients_match_oracle(shape):
     n, H, W = shape
     rng = np.random.default_rng(7)
     p = _params(11)
-    x = rng.normal(size=(n, H, W, 5)).astype(np.float32)
+    x = rng.normal(size=(n, H, W, cnn.DIMS[0][0])).astype(np.float32)
     gout = rng.normal(size=(n, H, W, 8)).astype(np.float32)
     ref = cnn.Net(p)
     y_ref = ref.forward(x)
@@ -71,7 +71,7 @@ def test_adam_reduces_a_regression_loss():
     import torch
     n, H, W = 2, 24, 130
     rng = np.random.default_rng(1)
-    x = rng.normal(size=(n, H, W, 5)).astype(np.float32)
+    x = rng.normal(size=(n, H, W, cnn.DIMS[0][0])).astype(np.float32)
     target = cnn.Net(_params(3)).forward(x).astype(np.float32)   # a reachable target
     dev = torch.device("cuda", 0)
     dx = torch.from_numpy(x).to(dev)
