@@ -209,6 +209,33 @@ int ouc_step_reconstruct(ouc_ctx* ctx, int t);
 int ouc_image_finalize(ouc_ctx* ctx, float* img_pp, float* img_ps);
 int ouc_step_fields(ouc_ctx* ctx, int side, float* fields);
 
+/* Survey on per-shot sub-grids (the batching form, no counterpart in the
+ * reference, which runs every shot on the whole grid, PS:2108).  Each shot k
+ * has an aperture: the interior columns [x0, x1) of the context's model that
+ * its sub-grid covers (its source column inside).  The sub-grid is the
+ * model's padded grid restricted to padded rows [x0, x1 + 2 npml): the
+ * absorbing cells on either side hold the model itself, and the damping
+ * profile is that of the sub-grid's own edges, so each shot equals a
+ * single-shot run of a context created on that window as a padded model.
+ * Shots are taken in the order given, up to cfg.max_batch per batch; the
+ * shots of a batch may differ in width and advance together (one launch per
+ * stage and time step, each CTA reading its shot's geometry).  Shot
+ * coordinates are interior coordinates of the whole model.
+ *   ouc_survey_forward: gathers per shot, (x1 - x0 + 2 npml) x nt each in
+ *     cfg.gather_layout (host; any pointer may be NULL).
+ *   ouc_survey_rtm: RTM of every shot (strip form only: snapshot_every = 0);
+ *     rec_vx/rec_vz as the forward gathers or NULL (self-modelled); images
+ *     (x1 - x0) x nz per shot (host, may be NULL); every image also enters
+ *     the context's FP64 stack at rows [x0, x1), shot by shot in order. */
+typedef struct ouc_aperture {
+    int x0, x1;             /* interior columns [x0, x1) of the model           */
+} ouc_aperture;
+int ouc_survey_forward(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_aperture* apertures,
+                       const float* wavelet, float* const* gather_vx, float* const* gather_vz);
+int ouc_survey_rtm(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_aperture* apertures,
+                   const float* wavelet, const float* const* rec_vx, const float* const* rec_vz, float* const* img_pp,
+                   float* const* img_ps);
+
 /* Forward modeling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they need
  * a modeling run: applications whose own memory pool owns the whole GPU and

@@ -28,6 +28,10 @@ class ouc_shot(C.Structure):
                 ("mute", C.c_int)]
 
 
+class ouc_aperture(C.Structure):
+    _fields_ = [("x0", C.c_int), ("x1", C.c_int)]
+
+
 class ouc_timing(C.Structure):
     _fields_ = [("forward_ms", C.c_float), ("backward_ms", C.c_float), ("finalize_ms", C.c_float),
                 ("copy_ms", C.c_float), ("kernel_launches", C.c_longlong)]
@@ -58,6 +62,10 @@ SIGNATURES = {
                                 C.POINTER(_fp), C.POINTER(_fp)]),
     "ouc_rtm_batch_dev": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), _vp, C.POINTER(_vp), C.POINTER(_vp),
                                     C.POINTER(_vp), C.POINTER(_vp)]),
+    "ouc_survey_forward": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), C.POINTER(ouc_aperture), _fp, C.POINTER(_fp),
+                                     C.POINTER(_fp)]),
+    "ouc_survey_rtm": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), C.POINTER(ouc_aperture), _fp, C.POINTER(_fp),
+                                 C.POINTER(_fp), C.POINTER(_fp), C.POINTER(_fp)]),
     "ouc_forward_noalloc": (C.c_int, [C.POINTER(ouc_config), C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
     "ouc_stack": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
     "ouc_stack_dev": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),

@@ -228,6 +228,59 @@ class Context:
         check(lib().ouc_rtm_batch_dev(self._h, n, sh, d_wavelet, arr(d_rx), arr(d_rz), arr(d_ipp), arr(d_ips)),
               self._h)
 
+    # -- survey on per-shot sub-grids (the batching form)
+    def _survey_args(self, shots, apertures):
+        n = len(shots)
+        if len(apertures) != n:
+            raise ValueError("one aperture (x0, x1) per shot")
+        sh = (_lib.ouc_shot * n)(*[s.c() for s in shots])
+        ap = (_lib.ouc_aperture * n)(*[_lib.ouc_aperture(int(a[0]), int(a[1])) for a in apertures])
+        return n, sh, ap
+
+    def _sub_gshape(self, ap):
+        Xb = ap[1] - ap[0] + 2 * self.cfg.npml
+        nt = self.cfg.nt
+        return (Xb, nt) if self.cfg.gather_layout == GATHER_XT else (nt, Xb)
+
+    def survey_forward(self, shots, apertures, wavelet):
+        """Forward modeling of shots on their sub-grids: apertures are interior
+        column ranges (x0, x1) of this model; returns [(gather_vx, gather_vz)],
+        each (x1 - x0 + 2 npml) wide."""
+        n, sh, ap = self._survey_args(shots, apertures)
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        out = [(np.zeros(self._sub_gshape(a), np.float32), np.zeros(self._sub_gshape(a), np.float32)) for a in apertures]
+        FP = C.POINTER(C.c_float)
+        gx = (FP * n)(*[_p(o[0]) for o in out])
+        gz = (FP * n)(*[_p(o[1]) for o in out])
+        check(lib().ouc_survey_forward(self._h, n, sh, ap, _p(w), gx, gz), self._h)
+        return out
+
+    def survey_rtm(self, shots, apertures, wavelet, recs=None):
+        """RTM of shots on their sub-grids; recs = [(rec_vx, rec_vz)] shaped as
+        survey_forward's gathers, or None (self-modelled).  Returns
+        [(img_pp, img_ps)], each (x1 - x0) x nz; all enter the FP64 stack."""
+        n, sh, ap = self._survey_args(shots, apertures)
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        FP = C.POINTER(C.c_float)
+        rx = rz = None
+        keep = []
+        if recs is not None:
+            ax_ = [_f32(r[0]) for r in recs]
+            az_ = [_f32(r[1]) for r in recs]
+            for a_, b_, apk in zip(ax_, az_, apertures):
+                assert a_.shape == self._sub_gshape(apk) and b_.shape == self._sub_gshape(apk)
+            keep += ax_ + az_
+            rx = (FP * n)(*[_p(a_) for a_ in ax_])
+            rz = (FP * n)(*[_p(a_) for a_ in az_])
+        imgs = [(np.zeros((a[1] - a[0], self.cfg.nz), np.float32), np.zeros((a[1] - a[0], self.cfg.nz), np.float32))
+                for a in apertures]
+        ipp = (FP * n)(*[_p(i[0]) for i in imgs])
+        ips = (FP * n)(*[_p(i[1]) for i in imgs])
+        check(lib().ouc_survey_rtm(self._h, n, sh, ap, _p(w), rx, rz, ipp, ips), self._h)
+        return imgs
+
     def forward_dev(self, shot: Shot, d_wavelet, d_gx=None, d_gz=None):
         sc = shot.c()
         check(lib().ouc_forward_dev(self._h, C.byref(sc), d_wavelet, d_gx, d_gz), self._h)

@@ -218,6 +218,13 @@ int upload_desc(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_wavel
                                   : nullptr;
         d[b].stage = ctx->stage ? ctx->stage + (size_t)b * 2 * ctx->strip_slot : nullptr;
         d[b].amax = ctx->amax ? ctx->amax + (size_t)b * ctx->nt * kStripFields : nullptr;
+        d[b].X = ctx->X;
+        d[b].tiles_x = ctx->tiles_x;
+        d[b].rec_tiles_x = ctx->rec_tiles_x;
+        d[b].ring = ctx->ring;
+        d[b].off = (size_t)b * ctx->shot_stride;
+        d[b].strip_slot = ctx->strip_slot;
+        d[b].vp2 = ctx->vp2; d[b].vs2 = ctx->vs2; d[b].ax = ctx->ax; d[b].az = ctx->az;
     }
     CK(cudaMemcpyAsync(ctx->d_desc, d.data(), n * sizeof(ShotDesc), cudaMemcpyHostToDevice, ctx->stream));
     return OUC_OK;
@@ -641,7 +648,7 @@ int ouc_destroy(ouc_ctx* ctx) {
     for (auto* p : ctx->d_stack) cudaFree(p);
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
-    cudaFree(ctx->l_in); cudaFree(ctx->l_out); cudaFree(ctx->l_truth); cudaFree(ctx->l_scale); cudaFree(ctx->l_tmp);
+    cudaFree(ctx->l_in); cudaFree(ctx->l_out); cudaFree(ctx->l_truth); cudaFree(ctx->l_scale); cudaFree(ctx->l_tmp); cudaFree(ctx->sv_model);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

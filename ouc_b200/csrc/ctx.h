@@ -80,6 +80,8 @@ struct ouc_ctx {
     float* l_truth = nullptr;    // restricted fine state, two levels [2][X][Z][4]
     float* l_scale = nullptr;    // [2] largest |U| and |U^n - U^(n-1)| of the state
     float* l_tmp = nullptr;      // [X][Z][OUC_CNN_OUT] smoothing scratch
+    // survey (survey.cu): per-slot sub-grid models [batch][4 fields] (vp2 vs2 ax az)
+    float* sv_model = nullptr;
     size_t bytes = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -109,6 +111,11 @@ int zero_side(ouc_ctx* ctx, int n, int side, bool with_acc);
 int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t);
 int run_forward(ouc_ctx* ctx, int n, bool record, bool save, bool snaps = false);
 int gather_out(ouc_ctx* ctx, const float* src_tx, float* dst, bool host);
+int gather_in(ouc_ctx* ctx, const float* src, float* dst_tx, bool host);
+int ensure_strips(ouc_ctx* ctx);
+int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src);
+void damping(const std::vector<float>& vp, int X, int Z, int L, double R, std::vector<float>& ax,
+             std::vector<float>& az);
 float elapsed(cudaEvent_t a, cudaEvent_t b);
 
 }  // namespace host

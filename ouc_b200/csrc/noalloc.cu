@@ -150,6 +150,13 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     desc.gather_x = gathers;
     desc.gather_z = gathers + (size_t)nt * X;
     desc.strips = nullptr;
+    desc.X = X;
+    desc.tiles_x = tiles_x;
+    desc.rec_tiles_x = tiles_x;
+    desc.ring = Ring::make(X, Z, L, N);
+    desc.off = 0;
+    desc.strip_slot = 0;
+    desc.vp2 = field(0); desc.vs2 = field(1); desc.ax = field(2); desc.az = field(3);
     if (cudaMemcpyAsync(d_desc, &desc, sizeof(desc), cudaMemcpyHostToDevice, stream) != cudaSuccess) return OUC_ECUDA;
 
     StepArgs a;

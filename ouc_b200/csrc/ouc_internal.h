@@ -83,6 +83,19 @@ struct ShotDesc {
     void* strips;                  // [slot][8 fields][ring] of the strip element type, or null
     float* stage;                  // kStripF16: staging ring [2][8 fields][ring] floats
     unsigned* amax;                // kStripF16: [slot][8 fields] bits of the largest |v| (float)
+    // Geometry of this shot's grid.  Shots of one launch share Z, L, N and
+    // the pitch but may differ in width (per-shot sub-grids of a survey); a
+    // CTA whose tile lies beyond its shot's width exits at once.
+    int X;                         // padded width (rows along x)
+    int tiles_x;                   // tile rows of the full step
+    int rec_tiles_x;               // tile rows of the reconstruction (interior)
+    Ring ring;                     // boundary ring of this grid
+    size_t off;                    // offset (floats) of this shot's fields from shot 0's
+    size_t strip_slot;             // floats per strip slot
+    const float* vp2;              // model views of this grid, cell (0, 0)
+    const float* vs2;
+    const float* ax;
+    const float* az;
 };
 
 struct StepArgs {
@@ -112,7 +125,8 @@ struct StepArgs {
     const float* rcv[4];              // receiver Px Pz Sx Sz after this back-step
     float* acc[3];                    // PP, PS, illumination accumulators
     float* comp[3];                   // their compensation terms (comp_image)
-    // model (shared by the batch)
+    // uniform geometry of the batch, for the kernels other than k_step
+    // (k_step reads each shot's geometry from its ShotDesc)
     const float* vp2;
     const float* vs2;
     const float* ax;
