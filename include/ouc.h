@@ -88,6 +88,9 @@ typedef struct ouc_config {
                                every K-th imaging level during the forward pass
                                and image only those levels (no reconstruction;
                                no counterpart in the reference)                 */
+    int use_graphs;         /* 1: capture each whole-shot time loop (one launch
+                               per stage and step) as a CUDA graph on first use
+                               and replay it for later shots and batches        */
 } ouc_config;
 
 typedef struct ouc_shot {
@@ -235,6 +238,18 @@ int ouc_survey_forward(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ou
 int ouc_survey_rtm(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_aperture* apertures,
                    const float* wavelet, const float* const* rec_vx, const float* const* rec_vz, float* const* img_pp,
                    float* const* img_ps);
+
+/* Autotuner of the launch batch (no counterpart in the reference): times
+ * `steps` forward steps of 1, 2, 4, ... and cfg.max_batch shots per launch on
+ * this context's grid (CUDA events; the wavelet buffer is cleared) and keeps
+ * the batch with the fewest ns per cell-update (a larger batch must be 3 %
+ * faster to win); *best_batch and *ns_per_cell may be NULL.  Later
+ * ouc_rtm_batch / ouc_survey_* calls advance that many shots per launch.
+ * ouc_set_run_batch sets it directly (1 .. cfg.max_batch), e.g. from a cache
+ * of earlier tuning results.  The tile shape (32 x 64 cells per CTA) is fixed
+ * at compile time. */
+int ouc_tune_batch(ouc_ctx* ctx, int steps, int* best_batch, float* ns_per_cell);
+int ouc_set_run_batch(ouc_ctx* ctx, int n);
 
 /* Forward modeling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they need

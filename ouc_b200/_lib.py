@@ -20,7 +20,8 @@ class ouc_config(C.Structure):
                 ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("nt", C.c_int), ("pml_r", C.c_double),
                 ("model_layout", C.c_int), ("strip_level", C.c_int), ("image_align", C.c_int),
                 ("strip_precision", C.c_int), ("compensated_image", C.c_int), ("gather_layout", C.c_int),
-                ("device", C.c_int), ("stream", C.c_void_p), ("max_batch", C.c_int), ("snapshot_every", C.c_int)]
+                ("device", C.c_int), ("stream", C.c_void_p), ("max_batch", C.c_int), ("snapshot_every", C.c_int),
+                ("use_graphs", C.c_int)]
 
 
 class ouc_shot(C.Structure):
@@ -66,6 +67,8 @@ SIGNATURES = {
                                      C.POINTER(_fp)]),
     "ouc_survey_rtm": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), C.POINTER(ouc_aperture), _fp, C.POINTER(_fp),
                                  C.POINTER(_fp), C.POINTER(_fp), C.POINTER(_fp)]),
+    "ouc_tune_batch": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "ouc_set_run_batch": (C.c_int, [_vp, C.c_int]),
     "ouc_forward_noalloc": (C.c_int, [C.POINTER(ouc_config), C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
     "ouc_stack": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
     "ouc_stack_dev": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),

@@ -256,10 +256,53 @@ int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t) {
     return OUC_OK;
 }
 
+// Run `body` (a whole-shot time loop that enqueues work on the context
+// stream and may set ctx->src) directly, or, with cfg.use_graphs, as a CUDA
+// graph: captured on first use for its key and replayed afterwards.  Every
+// launch argument of a loop depends only on the key and on fixed context
+// buffers (per-batch values travel in the shot descriptors), so one graph
+// serves every batch with that key.
+template <class F>
+int with_graph(ouc_ctx* ctx, const int (&key)[6], F&& body) {
+    if (!ctx->cfg.use_graphs) return body();
+    for (const auto& g : ctx->graphs) {
+        if (std::equal(key, key + 6, g.key)) {
+            CK(cudaGraphLaunch(g.exec, ctx->stream));
+            ctx->src = g.src_end;
+            ctx->timing.kernel_launches += g.launches;
+            return OUC_OK;
+        }
+    }
+    const long long before = ctx->timing.kernel_launches;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc ? rc : cuda_fail(ctx, e, "graph capture");
+    }
+    ouc_ctx::Graph g;
+    std::copy(key, key + 6, g.key);
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return cuda_fail(ctx, ei, "graph instantiation");
+    g.src_end = ctx->src;
+    g.launches = ctx->timing.kernel_launches - before;
+    ctx->graphs.push_back(g);
+    CK(cudaGraphLaunch(g.exec, ctx->stream));
+    return OUC_OK;
+}
+
 // Forward time loop (PS:2258-2292) of n shots.  Records into the time-major
 // gathers when `record`, saves the boundary ring of every step when `save`.
 int run_forward(ouc_ctx* ctx, int n, bool record, bool save, bool snaps) {
-    Side s = ctx->src;
+    const int key[6] = {0, n, record, save, snaps, 0};
+    return with_graph(ctx, key, [&]() { return run_forward_loop(ctx, n, record, save, snaps); });
+}
+
+int run_forward_loop(ouc_ctx* ctx, int n, bool record, bool save, bool snaps) {
+    Side s = ctx->src0;   // state zeroed below: start from the fixed buffer assignment
     int rc = zero_side(ctx, n, 0, false);
     if (rc) return rc;
     StepArgs a = base_args(ctx);
@@ -341,8 +384,13 @@ int rec_step(ouc_ctx* ctx, StepArgs& as, Side& s, const Side& r, int n, int t, b
 // Backward loop (PS:2313-2364) and imaging of n shots; the source side
 // holds the forward's last two levels on entry.
 int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
-    Side s = ctx->src;
-    Side r = ctx->rcv;
+    const int key[6] = {1, n, exact_strips, theta_src, 0, 0};
+    return with_graph(ctx, key, [&]() { return run_backward_loop(ctx, n, exact_strips, theta_src); });
+}
+
+int run_backward_loop(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
+    Side s = ctx->src;    // the forward's last two levels
+    Side r = ctx->rcv0;
     int rc = zero_side(ctx, n, 1, true);
     if (rc) return rc;
     StepArgs ar = rcv_args(ctx);
@@ -358,7 +406,12 @@ int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
 // Backward loop of the snapshot form: receiver back-propagation at every
 // step, imaging at the snapshot levels only.
 int run_backward_snap(ouc_ctx* ctx, int n) {
-    Side r = ctx->rcv;
+    const int key[6] = {2, n, 0, 0, 0, 0};
+    return with_graph(ctx, key, [&]() { return run_backward_snap_loop(ctx, n); });
+}
+
+int run_backward_snap_loop(ouc_ctx* ctx, int n) {
+    Side r = ctx->rcv0;
     int rc = zero_side(ctx, n, 1, true);
     if (rc) return rc;
     StepArgs ar = rcv_args(ctx);
@@ -510,6 +563,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->N = N; ctx->L = L; ctx->nx = cfg->nx; ctx->nz = cfg->nz; ctx->nt = cfg->nt;
     ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
     ctx->batch = std::max(1, cfg->max_batch);
+    ctx->run_batch = ctx->batch;
     for (int k = 0; k < N; ++k) ctx->a[k] = (float)kWeights[N][k];
     const int X = ctx->X, Z = ctx->Z;
 
@@ -628,6 +682,9 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     }
     for (int q = 0; q < 3; ++q) ctx->acc[q] = ctx->field(ctx->state, k++);
     for (int q = 0; q < 3; ++q) ctx->comp[q] = ctx->field(ctx->state, k++);
+    ctx->src0 = ctx->src;
+    ctx->rcv0 = ctx->rcv;
+    configure_step_kernels(N);   // kernel attributes set before any graph capture
     int rc = OUC_OK;
     if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
         (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data()))) {
@@ -649,6 +706,7 @@ int ouc_destroy(ouc_ctx* ctx) {
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
     cudaFree(ctx->l_in); cudaFree(ctx->l_out); cudaFree(ctx->l_truth); cudaFree(ctx->l_scale); cudaFree(ctx->l_tmp); cudaFree(ctx->sv_model);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -784,8 +842,8 @@ static int rtm_batch_impl(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const
         CK(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
         d_w = ctx->d_wavelet;
     }
-    for (int s0 = 0; s0 < nshots; s0 += ctx->batch) {
-        const int n = std::min(ctx->batch, nshots - s0);
+    for (int s0 = 0; s0 < nshots; s0 += ctx->run_batch) {
+        const int n = std::min(ctx->run_batch, nshots - s0);
         rc = rtm_group(ctx, n, shots + s0, d_w, rx ? rx + s0 : nullptr, rz ? rz + s0 : nullptr, ipp ? ipp + s0 : nullptr,
                        ips ? ips + s0 : nullptr, host);
         if (rc) return rc;

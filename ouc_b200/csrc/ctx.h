@@ -37,7 +37,8 @@ struct ouc_ctx {
     ouc_config cfg;
     int X = 0, Z = 0, L = 0, N = 0, nx = 0, nz = 0, nt = 0;
     int Xc = 0, Zc = 0, pitch = 0;
-    int batch = 1;               // shots per launch
+    int batch = 1;               // shots the device state holds (cfg.max_batch)
+    int run_batch = 1;           // shots advanced per launch (<= batch; ouc_tune_batch)
     size_t fstride = 0;          // floats per field allocation
     size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;
@@ -56,6 +57,16 @@ struct ouc_ctx {
     float* state = nullptr;      // batch shot blocks
     float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
     Side src{}, rcv{};
+    Side src0{}, rcv0{};         // leapfrog buffer assignment the whole-shot loops start from
+    // CUDA graphs of whole-shot time loops (cfg.use_graphs), keyed by loop
+    // kind and flags; replayed for every later batch with the same key
+    struct Graph {
+        int key[6];
+        cudaGraphExec_t exec;
+        Side src_end;            // source side after the loop
+        long long launches;      // kernels in the loop
+    };
+    std::vector<Graph> graphs;
     float* acc[3] = {nullptr, nullptr, nullptr};
     float* comp[3] = {nullptr, nullptr, nullptr};   // compensation terms of acc (compensated_image)
     float* gathers = nullptr;    // [batch][2][nt][X], time-major
@@ -110,10 +121,13 @@ int zero_side(ouc_ctx* ctx, int n, int side, bool with_acc);
 // One forward step of n shots at time t; swaps the leapfrog levels of `s`.
 int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t);
 int run_forward(ouc_ctx* ctx, int n, bool record, bool save, bool snaps = false);
+int run_forward_loop(ouc_ctx* ctx, int n, bool record, bool save, bool snaps);
 int gather_out(ouc_ctx* ctx, const float* src_tx, float* dst, bool host);
 int gather_in(ouc_ctx* ctx, const float* src, float* dst_tx, bool host);
 int ensure_strips(ouc_ctx* ctx);
 int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src);
+int run_backward_loop(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src);
+int run_backward_snap_loop(ouc_ctx* ctx, int n);
 void damping(const std::vector<float>& vp, int X, int Z, int L, double R, std::vector<float>& ax,
              std::vector<float>& az);
 float elapsed(cudaEvent_t a, cudaEvent_t b);

@@ -11,13 +11,33 @@
 namespace ouc {
 
 template <int N, int MODE>
+static void configure_one() {
+    constexpr int bytes = TileGeo<N>::bytes;
+    cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+}
+
+template <int N>
+static void configure_modes() {
+    configure_one<N, kFwd>();
+    configure_one<N, kRcv>();
+    configure_one<N, kRec>();
+}
+
+// Shared-memory attributes of the step kernels of half-order N, set once per
+// process (and per device the caller makes current) before their first launch.
+void configure_step_kernels(int N) {
+    if (N == 2) configure_modes<2>();
+    if (N == 5) configure_modes<5>();
+    if (N == 6) configure_modes<6>();
+}
+
+template <int N, int MODE>
 static void launch_one(const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
     constexpr int bytes = TileGeo<N>::bytes;
-    static bool configured = false;   // one attribute call per instantiation
+    static bool configured = false;   // one attribute call per instantiation (callers outside a context)
     if (!configured) {
-        cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
+        configure_one<N, MODE>();
         configured = true;
     }
     k_step<N, MODE><<<dim3(tiles_x * a.tiles_z, nshots), kThreads, bytes, s>>>(a);

@@ -175,6 +175,7 @@ struct SnapArgs {
 
 // Host-side launchers (kernels.cu)
 int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s);
+void configure_step_kernels(int N);
 int step_smem_bytes(int N);
 void launch_image_only(const StepArgs& a, int nshots, cudaStream_t s);
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s);

@@ -284,6 +284,7 @@ int main(int argc, char** argv) {
     cfg.gather_layout = OUC_GATHER_XT;
     cfg.device = r.device;
     cfg.max_batch = r.batch;
+    cfg.use_graphs = 1;
 
     std::vector<float> wavelet(r.nt);
     int t0 = 0;

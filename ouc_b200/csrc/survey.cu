@@ -240,8 +240,8 @@ int run(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_aperture* ap,
     if (!forward_only && (rc = ensure_strips(ctx))) return rc;
     ctx->timing = ouc_timing{};
     CKS(cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream));
-    for (int s0 = 0; s0 < nshots; s0 += ctx->batch) {
-        const int n = std::min(ctx->batch, nshots - s0);
+    for (int s0 = 0; s0 < nshots; s0 += ctx->run_batch) {
+        const int n = std::min(ctx->run_batch, nshots - s0);
         auto sub = [&](auto* p) { return p ? p + s0 : nullptr; };
         rc = group(ctx, n, shots + s0, ap + s0, ctx->d_wavelet, forward_only, sub(gx), sub(gz), sub(rx), sub(rz),
                    sub(ipp), sub(ips));
@@ -250,10 +250,65 @@ int run(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_aperture* ap,
     return OUC_OK;
 }
 
+// Forward steps per second of n copies of a centre shot (CUDA events).
+int time_batch(ouc_ctx* ctx, int n, int steps, float* ms) {
+    std::vector<ouc_shot> shots(n);
+    for (auto& s : shots) {
+        memset(&s, 0, sizeof(s));
+        s.sx = ctx->nx / 2; s.sz = std::min(2, ctx->nz - 1); s.rz = s.sz;
+    }
+    int rc = upload_desc(ctx, n, shots.data(), ctx->d_wavelet);
+    if (rc || (rc = zero_side(ctx, n, 0, false))) return rc;
+    Side s = ctx->src0;
+    StepArgs a = base_args(ctx);
+    for (int t = 0; t < 2; ++t)
+        if ((rc = fwd_step(ctx, a, s, n, t))) return rc;
+    CKS(cudaEventRecord(ctx->ev[0], ctx->stream));
+    for (int t = 2; t < 2 + steps; ++t)
+        if ((rc = fwd_step(ctx, a, s, n, t % ctx->nt))) return rc;
+    CKS(cudaEventRecord(ctx->ev[1], ctx->stream));
+    CKS(cudaStreamSynchronize(ctx->stream));
+    *ms = elapsed(ctx->ev[0], ctx->ev[1]);
+    return OUC_OK;
+}
+
 }  // namespace survey
 }  // namespace ouc
 
 extern "C" {
+
+int ouc_tune_batch(ouc_ctx* ctx, int steps, int* best_batch, float* ns_per_cell) {
+    if (!ctx || steps < 1) return OUC_EINVAL;
+    cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;
+    if (cudaMemsetAsync(ctx->d_wavelet, 0, (size_t)ctx->nt * 4, ctx->stream) != cudaSuccess) return OUC_ECUDA;
+    std::vector<int> cands;
+    for (int n = 1; n < ctx->batch; n *= 2) cands.push_back(n);
+    cands.push_back(ctx->batch);
+    int best = 1;
+    float best_ns = 0.f;
+    for (int n : cands) {
+        float ms = 0.f;
+        int rc = ouc::survey::time_batch(ctx, n, steps, &ms);
+        if (rc) return rc;
+        const float ns = ms * 1e6f / ((float)n * steps * ctx->X * ctx->Z);
+        // a larger batch must be clearly faster to be preferred (memory per shot)
+        if (best_ns == 0.f || ns < 0.97f * best_ns) {
+            best = n;
+            best_ns = ns;
+        }
+    }
+    ctx->run_batch = best;
+    if (best_batch) *best_batch = best;
+    if (ns_per_cell) *ns_per_cell = best_ns;
+    return OUC_OK;
+}
+
+int ouc_set_run_batch(ouc_ctx* ctx, int n) {
+    if (!ctx || n < 1 || n > ctx->batch) return OUC_EINVAL;
+    ctx->run_batch = n;
+    return OUC_OK;
+}
 
 int ouc_survey_forward(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_aperture* apertures,
                        const float* wavelet, float* const* gather_vx, float* const* gather_vz) {
