@@ -167,6 +167,71 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_survey(args, rank, world):
+    """Batched uneven-shot RTM (the c3 survey): each step migrates one batch of
+    shots on their own sub-grids through ouc_survey_rtm (host records in,
+    per-shot images out, copies inside the timed region).  One GPU."""
+    import torch
+    import ouc_b200 as o
+    from ouc_b200 import models, tuning
+    if world > 1:
+        raise SystemExit("the survey workload runs on one GPU")
+    torch.cuda.set_device(0)
+    w = models.c3(nt=args.nt) if args.nt else models.c3()
+    cfg = w.cfg
+    B = max(1, args.batch)
+    cfg.max_batch = B
+    cfg.strip_precision = {"fp32": o.PREC_FP32, "fp16": o.PREC_FP16, "bf16": o.PREC_BF16}[args.strips]
+    wavelet, t0 = o.ricker(w.fm, cfg.dt, cfg.nt)
+    shots = [o.Shot(s.sx, s.sz, s.rz, t0=t0) for s in w.shots]
+    # one batch of shots spread over the survey (every len/B-th shot)
+    pick = list(range(0, len(shots), max(1, len(shots) // B)))[:B]
+    sh = [shots[k] for k in pick]
+    aps = [w.apertures[k] for k in pick]
+    true_ctx = o.Context(cfg, w.vp, w.vs, w.rho)
+    recs = true_ctx.survey_forward(sh, aps, wavelet)          # acquisition, not timed
+    true_ctx.close()
+    pin = [(torch.from_numpy(r[0]).pin_memory().numpy(), torch.from_numpy(r[1]).pin_memory().numpy()) for r in recs]
+    mig = o.Context(cfg, w.vp_mig, w.vs_mig, w.rho)
+    tuned, ns_cell, cached = tuning.tune(mig, steps=10)
+    for _ in range(args.warmup):
+        mig.survey_rtm(sh, aps, wavelet, pin)
+    clocks = Clocks(0)
+    times, fwd, bwd = [], [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        mig.survey_rtm(sh, aps, wavelet, pin)
+        times.append(time.perf_counter() - t1)
+        t = mig.timing()
+        fwd.append(t["forward_ms"])
+        bwd.append(t["backward_ms"])
+    clk = clocks.stop()
+    launches = mig.timing()["kernel_launches"]
+    mig.close()
+    s_step = statistics.median(times)
+    L = cfg.npml
+    cells = sum(cfg.nt * (2 * (x1 - x0 + 2 * L) * cfg.Z + (x1 - x0) * cfg.nz) for x0, x1 in aps)
+    value = cells / s_step / 1e9
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * s_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded folded model, modelled records)",
+                "config": {"workload": w.name, "model": [cfg.nx, cfg.nz], "nt": cfg.nt, "dx_m": cfg.dx,
+                           "dt_s": cfg.dt, "shots_per_step": len(sh), "apertures": aps, "strips": args.strips,
+                           "step": "one batch of uneven sub-grid RTM shots, host records in, images out",
+                           "launch_batch": tuned, "tuned_ns_per_cell_update": ns_cell, "tuning_cached": cached,
+                           "graphs": True, "l2": "per-step working set of the batch exceeds L2"},
+                "shots_per_hour": 3600.0 * len(sh) / s_step,
+                "phase_ms": {"forward": statistics.median(fwd), "backward": statistics.median(bwd)},
+                "e2e": {"value": value, "unit": UNIT,
+                        "h2d_bytes_per_step": sum(2 * r[0].size * 4 for r in recs) + cfg.nt * 4,
+                        "d2h_bytes_per_step": sum(2 * (x1 - x0) * cfg.nz * 4 for x0, x1 in aps)},
+                "gpu_launches": int(launches), "clocks": clk}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -174,10 +239,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ouc", choices=["ouc", "reference"])
     ap.add_argument("--nt", type=int, default=None, help="time steps per shot (default: the workload's)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
                     help="c2: the headline 1000x500 RTM workload; c4: the 4000x1500 grid (HBM-bound profiling)")
     ap.add_argument("--ref-steps", type=int, default=None, help="CPU sample length (time steps)")
-    ap.add_argument("--batch", type=int, default=16, help="shots advanced together per step")
+    ap.add_argument("--batch", type=int, default=16, help="shots advanced together per step (c3: shots per step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--strips", default="fp32", choices=["fp32", "fp16", "bf16"],
                     help="boundary-strip storage (fp16: scaled per slot and field)")
@@ -192,6 +257,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "c3":
+        return run_survey(args, rank, world)
 
     import torch
     import torch.distributed as dist

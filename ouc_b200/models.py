@@ -27,6 +27,7 @@ class Workload:
     shots: list = field(default_factory=list)
     vp_mig: np.ndarray | None = None   # migration model (None: the true model)
     vs_mig: np.ndarray | None = None
+    apertures: list | None = None      # per-shot sub-grids: interior columns (x0, x1)
 
     def cell_updates_per_shot(self, rtm=True):
         """Cell-updates of one shot: forward and receiver on the padded grid,
@@ -136,6 +137,26 @@ def c2(nt=4000, seed=1236, nshots=40):
     shots = [Shot(int(x), 2, 2) for x in xs]
     return Workload("c2_rtm_1000x500_nt4000", cfg, vp, vs, rho, 25.0, shots,
                     gaussian_smooth(vp, 10.0), gaussian_smooth(vs, 10.0))
+
+
+def c3(nt=6000, seed=1237, nshots=256):
+    """Batched uneven-shot RTM: 2000 x 800 interior, dx = 5 m, 30-cell CPML;
+    folded layers with 3 faults and 20 velocity anomalies (+/-10 %); 256
+    shots on z = 2, each on its own sub-grid: a receiver aperture of U[400,
+    1600] cells centred on the source (shifted inside the model); 30 Hz,
+    dt = 0.4 ms, nt = 6000; migration model Gaussian-smoothed (sigma = 10)."""
+    rng = np.random.default_rng(seed)
+    vp, vs, rho = folded_model(2000, 800, rng)
+    cfg = Config(nx=2000, nz=800, npml=30, dx=5.0, dz=5.0, dt=4e-4, nt=nt, half_order=5)
+    xs = np.linspace(0, 1999, nshots).round().astype(int)
+    widths = rng.uniform(400, 1600, nshots).round().astype(int)
+    shots, aps = [], []
+    for x, a in zip(xs, widths):
+        x0 = int(max(0, min(x - a // 2, 2000 - a)))
+        shots.append(Shot(int(x), 2, 2))
+        aps.append((x0, x0 + int(a)))
+    return Workload("c3_survey_2000x800_nt6000", cfg, vp, vs, rho, 30.0, shots, gaussian_smooth(vp, 10.0),
+                    gaussian_smooth(vs, 10.0), aps)
 
 
 def c4(nt=8000, seed=1238, nshots=128):
