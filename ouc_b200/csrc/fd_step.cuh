@@ -194,6 +194,7 @@ __device__ __forceinline__ void dx4(const float* col, int st, const float* a, co
 
 // Per-launch, per-shot constants.
 struct ShotView {
+    int b;                 // shot of the batch
     int sx, sz, rz, src_type;
     const float* wavelet;
     float* rec_x;          // gather row t (kFwd) or nullptr
@@ -223,6 +224,7 @@ __device__ __forceinline__ Geo geo_of(const ShotDesc& d) {
 __device__ __forceinline__ ShotView shot_view(const StepArgs& p, int b) {
     const ShotDesc& d = p.shots[b];
     ShotView v;
+    v.b = b;
     v.sx = d.sx; v.sz = d.sz; v.rz = d.rz; v.src_type = d.src_type;
     v.wavelet = d.wavelet;
     v.rec_x = p.record ? d.gather_x + (size_t)p.t * d.X : nullptr;
@@ -374,6 +376,46 @@ __device__ __forceinline__ bool u_live(const StepArgs& p, const Geo& gm, int gi,
     return gi >= N && gi < gm.X - N && gj >= N && gj < p.Z - N;
 }
 
+// L2 prefetch of a tile's operands, one 128-byte line per instruction, so
+// that the loads of the three phases find their lines in flight or resident:
+// the U box of phase 1 (current level, 4 fields), the oldest level (read and
+// overwritten in phase 3) and, for the reconstruction, the receiver level and
+// the imaging accumulators over the own cells, and the model over the S
+// region (phase 2).  Every address lies inside the field allocations (guard
+// rows and columns included).
+template <int N, int MODE>
+__device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, size_t off, int x0, int z0) {
+    using G = TileGeo<N>;
+    constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS, HU = G::HU;
+    const int tid = threadIdx.x;
+    const int P = p.pitch;
+    const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;
+    constexpr int kUPer = (G::UC + 16 + 31) / 32;   // the box starts 16 floats into a line
+    constexpr int kULines = G::UR * kUPer;
+    for (int k = tid; k < 4 * kULines; k += kThreads) {
+        const int f = k / kULines, l = k - f * kULines;
+        const ptrdiff_t g = (ptrdiff_t)(ux_i0 + l / kUPer) * P + ux_j0 + 32 * (l % kUPer);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p.now[f] + off + g));
+    }
+    constexpr int kOwnLines = TX * (TZ / 32);
+    for (int k = tid; k < 4 * kOwnLines; k += kThreads) {
+        const int f = k / kOwnLines, l = k - f * kOwnLines;
+        const ptrdiff_t g = (ptrdiff_t)(x0 + l / (TZ / 32)) * P + z0 + 32 * (l % (TZ / 32));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p.past[f] + off + g));
+        if (MODE == kRec) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(p.rcv[f] + off + g));
+            if (f < 3) asm volatile("prefetch.global.L2 [%0];" ::"l"(p.acc[f] + off + g));
+        }
+    }
+    constexpr int kSPer = (TZ + 2 * HS + 31) / 32 + 1;
+    constexpr int kSLines = (TX + 2 * SHX) * kSPer;
+    for (int k = tid; k < 2 * kSLines; k += kThreads) {
+        const int f = k / kSLines, l = k - f * kSLines;
+        const ptrdiff_t g = (ptrdiff_t)(x0 - SHX + l / kSPer) * P + (z0 - HS) + 32 * (l % kSPer);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"((f ? gm.vs2 : gm.vp2) + g));
+    }
+}
+
 template <int N, int MODE>
 __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, const ShotView& sv, float* sm, int x0, int z0,
                                           const TileFlags& f) {
@@ -421,7 +463,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
     if (MODE == kRec && f.ring) {
         __syncthreads();
         // reconstruction: the ring comes from the saved strips (read_wavefiled1, PS:1344-1376)
-        const ShotDesc& d = p.shots[blockIdx.y];
+        const ShotDesc& d = p.shots[sv.b];
         const void* su = strip_slot_ptr(p, d, p.slot_u);
         const unsigned* am = d.amax ? d.amax + (size_t)p.slot_u * kStripFields : nullptr;
         for_ring(gm.ring, ux_i0, ux_i0 + G::UR, ux_j0, ux_j0 + UC, [&](int i, int j, int ri) {
@@ -533,7 +575,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
     }
     if (f.ring) {
         __syncthreads();
-        const ShotDesc& d = p.shots[blockIdx.y];
+        const ShotDesc& d = p.shots[sv.b];
         if (MODE == kRec) {
             // read_wavefiled2 (PS:1377-1424): theta, omega and the Q fields of the ring
             const void* ss = strip_slot_ptr(p, d, p.slot_s);
@@ -728,7 +770,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
     if (MODE == kFwd && f.ring) {
         // save_wavefiled (PS:1230-1287): the new displacement of the tile's ring cells
         __syncthreads();
-        const ShotDesc& d = p.shots[blockIdx.y];
+        const ShotDesc& d = p.shots[sv.b];
         void* s = strip_save_ptr(p, d);
         float m[2] = {0.f, 0.f};
         for_ring(gm.ring, x0, x0 + TX, z0, z0 + TZ, [&](int i, int j, int ri) {
@@ -770,6 +812,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
     const int x0 = (p.tile_x0 + tx) * G::TX, z0 = (p.tile_z0 + tz) * G::TZ;
     const Geo gm = geo_of(d);
+    prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
     const ShotView sv = shot_view(p, blockIdx.y);
     const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
     step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f);
