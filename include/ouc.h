@@ -88,6 +88,12 @@ typedef struct ouc_config {
                                every K-th imaging level during the forward pass
                                and image only those levels (no reconstruction;
                                no counterpart in the reference)                 */
+    int density;            /* 1: variable density from the rho model (moduli
+                               rho Vp^2, rho Vs^2; acceleration = buoyancy x
+                               stress divergence, buoyancy averaged onto the
+                               staggered Ux/Uz positions); 0: the reference's
+                               density-normalised equations, rho ignored (no
+                               counterpart in the reference for 1)             */
     int use_graphs;         /* 1: capture each whole-shot time loop (one launch
                                per stage and step) as a CUDA graph on first use
                                and replay it for later shots and batches        */
@@ -127,7 +133,7 @@ int ouc_ricker(float fm, float dt, int nt, float* out, int* t0);
  * (xiangbian, PS:37-119), builds the damping profile (PS:2067-2105) and
  * allocates all device state.  vp/vs/rho are nx*nz (OUC_MODEL_INTERIOR) or
  * X*Z (OUC_MODEL_PADDED); rho may be NULL and is not used by the
- * reference's density-normalised equations (PS:373-378). */
+ * reference's density-normalised equations (PS:373-378) unless cfg->density. */
 int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const float* rho, ouc_ctx** out);
 int ouc_destroy(ouc_ctx* ctx);
 int ouc_dims(const ouc_ctx* ctx, int* X, int* Z);

@@ -102,10 +102,17 @@ struct Wave {
     }
 };
 
+// Model.  With `dens` (the variable-density extension, no counterpart in the
+// reference, whose equations are density-normalised, PS:373-378) the moduli
+// are rho Vp^2 and rho Vs^2 and each displacement component's acceleration is
+// scaled by the buoyancy 1/rho averaged onto its staggered position:
+// bx(i, j) = (1/rho(i, j) + 1/rho(i+1, j)) / 2 for Ux, bz likewise along z.
 template <class T>
 struct Model {
     int X, Z;
     Field<T> vp, vs, ax, az;
+    bool dens = false;
+    Field<T> rho, bx, bz;
 };
 
 // S-stage at one cell: the four strain-like derivatives of U, the CPML
@@ -125,6 +132,10 @@ inline void s_cell(Wave<T>& w, const Model<T>& m, const T* a, int N, T dx, T dz,
     T ezx = dplus(UZ, (ptrdiff_t)Z, a, N, dx);    // dvzdx
     T vp2 = m.vp.v[c] * m.vp.v[c];
     T vs2 = m.vs.v[c] * m.vs.v[c];
+    if (m.dens) {
+        vp2 = vp2 * m.rho.v[c];
+        vs2 = vs2 * m.rho.v[c];
+    }
     if (PML) {
         T ax = m.ax.v[c], az = m.az.v[c];
         T fxx = w.fxx.v[c] = cpml(w.fxx.v[c], ax, exx, dt);
@@ -186,10 +197,18 @@ inline void u_cell(Wave<T>& w, const Model<T>& m, const T* a, int N, T dx, T dz,
     T oWz = w.oWz.v[c] = cpml(w.oWz.v[c], az, d.wz, dt);
     T oWx = w.oWx.v[c] = cpml(w.oWx.v[c], ax, d.wx, dt);
     const T dt2 = dt * dt;
-    T npx = 2 * w.pnx.v[c] - w.ppx.v[c] + dt2 * (d.tx - oTx + d.C - d.E - oC + oE);
-    T npz = 2 * w.pnz.v[c] - w.ppz.v[c] + dt2 * (d.tz - oTz + d.B - d.A - oB + oA);
-    T nsx = 2 * w.snx.v[c] - w.spx.v[c] + dt2 * (d.wz - oWz + d.C - d.E - oC + oE);
-    T nsz = 2 * w.snz.v[c] - w.spz.v[c] + dt2 * (-d.wx + oWx + d.B - d.A - oB + oA);
+    T spx = d.tx - oTx + d.C - d.E - oC + oE;
+    T spz = d.tz - oTz + d.B - d.A - oB + oA;
+    T ssx = d.wz - oWz + d.C - d.E - oC + oE;
+    T ssz = -d.wx + oWx + d.B - d.A - oB + oA;
+    if (m.dens) {
+        spx = spx * m.bx.v[c]; ssx = ssx * m.bx.v[c];
+        spz = spz * m.bz.v[c]; ssz = ssz * m.bz.v[c];
+    }
+    T npx = 2 * w.pnx.v[c] - w.ppx.v[c] + dt2 * spx;
+    T npz = 2 * w.pnz.v[c] - w.ppz.v[c] + dt2 * spz;
+    T nsx = 2 * w.snx.v[c] - w.spx.v[c] + dt2 * ssx;
+    T nsz = 2 * w.snz.v[c] - w.spz.v[c] + dt2 * ssz;
     w.ppx.v[c] = w.pnx.v[c]; w.pnx.v[c] = npx;
     w.ppz.v[c] = w.pnz.v[c]; w.pnz.v[c] = npz;
     w.spx.v[c] = w.snx.v[c]; w.snx.v[c] = nsx;
@@ -202,8 +221,8 @@ inline void u_cell(Wave<T>& w, const Model<T>& m, const T* a, int N, T dx, T dz,
 // the value of "now" before the level shift (the reference passes d_Vpx_s
 // etc. there, which the imaging condition reads afterwards).
 template <class T>
-inline void u_cell_reverse(Wave<T>& w, Field<T>* prev, const T* a, int N, T dx, T dz, T dt, int i,
-                           int j) {
+inline void u_cell_reverse(Wave<T>& w, const Model<T>& m, Field<T>* prev, const T* a, int N, T dx, T dz, T dt,
+                           int i, int j) {
     const size_t c = (size_t)i * w.Z + j;
     UDerivs<T> d = u_derivs(w, a, N, dx, dz, c);
     const T dt2 = dt * dt;
@@ -211,10 +230,15 @@ inline void u_cell_reverse(Wave<T>& w, Field<T>* prev, const T* a, int N, T dx, 
     prev[0].v[c] = qpx; prev[1].v[c] = qpz; prev[2].v[c] = qsx; prev[3].v[c] = qsz;
     w.pnx.v[c] = w.ppx.v[c]; w.pnz.v[c] = w.ppz.v[c];
     w.snx.v[c] = w.spx.v[c]; w.snz.v[c] = w.spz.v[c];
-    T npx = 2 * w.pnx.v[c] - qpx + dt2 * (d.tx + d.C - d.E);
-    T npz = 2 * w.pnz.v[c] - qpz + dt2 * (d.tz + d.B - d.A);
-    T nsx = 2 * w.snx.v[c] - qsx + dt2 * (d.wz + d.C - d.E);
-    T nsz = 2 * w.snz.v[c] - qsz + dt2 * (-d.wx + d.B - d.A);
+    T spx = d.tx + d.C - d.E, spz = d.tz + d.B - d.A, ssx = d.wz + d.C - d.E, ssz = -d.wx + d.B - d.A;
+    if (m.dens) {
+        spx = spx * m.bx.v[c]; ssx = ssx * m.bx.v[c];
+        spz = spz * m.bz.v[c]; ssz = ssz * m.bz.v[c];
+    }
+    T npx = 2 * w.pnx.v[c] - qpx + dt2 * spx;
+    T npz = 2 * w.pnz.v[c] - qpz + dt2 * spz;
+    T nsx = 2 * w.snx.v[c] - qsx + dt2 * ssx;
+    T nsz = 2 * w.snz.v[c] - qsz + dt2 * ssz;
     w.ppx.v[c] = npx; w.ppz.v[c] = npz; w.spx.v[c] = nsx; w.spz.v[c] = nsz;
     w.ux.v[c] = npx + nsx;
     w.uz.v[c] = npz + nsz;
@@ -285,7 +309,8 @@ struct Engine {
     T dx, dz, dt;
     Model<T> m;
 
-    void setup(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az) {
+    void setup(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+               const float* rho = nullptr) {
         cfg = *c;
         X = c->X; Z = c->Z; L = c->L; N = c->N;
         for (int k = 0; k < 8; ++k) a[k] = (T)c->coeff[k];
@@ -295,6 +320,19 @@ struct Engine {
         for (size_t k = 0; k < (size_t)X * Z; ++k) {
             m.vp.v[k] = (T)vp[k]; m.vs.v[k] = (T)vs[k];
             m.ax.v[k] = (T)ax[k]; m.az.v[k] = (T)az[k];
+        }
+        m.dens = rho != nullptr;
+        if (m.dens) {
+            for (Field<T>* f : {&m.rho, &m.bx, &m.bz}) f->init(X, Z);
+            for (int i = 0; i < X; ++i)
+                for (int j = 0; j < Z; ++j) {
+                    const size_t k = (size_t)i * Z + j;
+                    const double b = 1.0 / rho[k];
+                    const double bxn = i + 1 < X ? 1.0 / rho[k + Z] : b, bzn = j + 1 < Z ? 1.0 / rho[k + 1] : b;
+                    m.rho.v[k] = (T)rho[k];
+                    m.bx.v[k] = (T)(0.5 * (b + bxn));
+                    m.bz.v[k] = (T)(0.5 * (b + bzn));
+                }
         }
     }
 
@@ -408,7 +446,7 @@ struct Engine {
                 // reshot_u (PS:2334) on the interior
 #pragma omp parallel for schedule(static)
                 for (int i = L; i < X - L; ++i)
-                    for (int j = L; j < Z - L; ++j) u_cell_reverse<T>(r, prev, a, N, dx, dz, dt, i, j);
+                    for (int j = L; j < Z - L; ++j) u_cell_reverse<T>(r, m, prev, a, N, dx, dz, dt, i, j);
                 // read_wavefiled1 (PS:2337): U strips; the reference reads slot t
                 int uslot = cfg.strip_level == 0 ? t : t - 1;
                 restore_bands(r, b, st, uslot, 0, 2);
@@ -482,9 +520,9 @@ struct Engine {
 
 template <class T>
 int run_forward(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
-                const float* src, T* rec_vx, T* rec_vz, T* fields_out) {
+                const float* src, T* rec_vx, T* rec_vz, T* fields_out, const float* rho = nullptr) {
     Engine<T> e;
-    e.setup(c, vp, vs, ax, az);
+    e.setup(c, vp, vs, ax, az, rho);
     Wave<T> w;
     w.init(c->X, c->Z);
     std::vector<T> rx((size_t)c->X * c->nt), rz((size_t)c->X * c->nt);
@@ -520,6 +558,20 @@ int orc_rtm_f64(const orc_cfg* c, const float* vp, const float* vs, const float*
                 double* raw_pp, double* raw_ps, double* acc, double* rec_out, double* fields_out) {
     Engine<double> e;
     e.setup(c, vp, vs, ax, az);
+    e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, raw_pp, raw_ps, acc, rec_out, fields_out);
+    return 0;
+}
+
+// Variable-density variants (rho: padded X x Z density; see Model).
+int orc_forward_rho_f64(const orc_cfg* c, const float* vp, const float* vs, const float* rho, const float* ax,
+                        const float* az, const float* src, double* rec_vx, double* rec_vz, double* fields_out) {
+    return run_forward<double>(c, vp, vs, ax, az, src, rec_vx, rec_vz, fields_out, rho);
+}
+int orc_rtm_rho_f64(const orc_cfg* c, const float* vp, const float* vs, const float* rho, const float* ax,
+                    const float* az, const float* src, const float* rec_x, const float* rec_z, double* lap_pp,
+                    double* lap_ps, double* raw_pp, double* raw_ps, double* acc, double* rec_out, double* fields_out) {
+    Engine<double> e;
+    e.setup(c, vp, vs, ax, az, rho);
     e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, raw_pp, raw_ps, acc, rec_out, fields_out);
     return 0;
 }

@@ -97,6 +97,11 @@ class Oracle:
             f = getattr(self.lib, name)
             f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, t, t, t, t, t, t, t]
             f.restype = C.c_int
+        self.lib.orc_forward_rho_f64.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _dp, _dp, _dp]
+        self.lib.orc_forward_rho_f64.restype = C.c_int
+        self.lib.orc_rtm_rho_f64.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _dp, _dp, _dp,
+                                             _dp, _dp, _dp, _dp]
+        self.lib.orc_rtm_rho_f64.restype = C.c_int
         self.lib.orc_pad_model.argtypes = [_fp, C.c_int, C.c_int, C.c_int]
         self.lib.orc_cpml_profile.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_double, _fp, _fp]
         self.lib.orc_num_threads.restype = C.c_int
@@ -119,21 +124,28 @@ class Oracle:
         self.lib.orc_cpml_profile(_ptr(vp), vp.shape[0], vp.shape[1], L, R, _ptr(ax), _ptr(az))
         return ax, az
 
-    def forward(self, shot: Shot, vp, vs, ax, az, src, fp64=False):
-        dt = np.float64 if fp64 else np.float32
+    def forward(self, shot: Shot, vp, vs, ax, az, src, fp64=False, rho=None):
+        """rho (padded density): the variable-density extension, FP64 only."""
+        dt = np.float64 if fp64 or rho is not None else np.float32
         X, Z, nt = shot.X, shot.Z, shot.nt
         rx = np.zeros((X, nt), dt)
         rz = np.zeros((X, nt), dt)
         fields = np.zeros((12, X, Z), dt)
-        f = self.lib.orc_forward_f64 if fp64 else self.lib.orc_forward_f32
         c = shot.cfg()
+        if rho is not None:
+            rc = self.lib.orc_forward_rho_f64(C.byref(c), _ptr(vp), _ptr(vs), _ptr(rho), _ptr(ax), _ptr(az), _ptr(src),
+                                              _ptr(rx, dt), _ptr(rz, dt), _ptr(fields, dt))
+            assert rc == 0
+            return rx, rz, fields
+        f = self.lib.orc_forward_f64 if fp64 else self.lib.orc_forward_f32
         rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx, dt), _ptr(rz, dt),
                _ptr(fields, dt))
         assert rc == 0
         return rx, rz, fields
 
-    def rtm(self, shot: Shot, vp, vs, ax, az, src, rec=None, fp64=False):
-        dt = np.float64 if fp64 else np.float32
+    def rtm(self, shot: Shot, vp, vs, ax, az, src, rec=None, fp64=False, rho=None):
+        """rho (padded density): the variable-density extension, FP64 only."""
+        dt = np.float64 if fp64 or rho is not None else np.float32
         X, Z, nt, L = shot.X, shot.Z, shot.nt, shot.L
         nx, nz = X - 2 * L, Z - 2 * L
         out = dict(lap_pp=np.zeros((nx, nz), dt), lap_ps=np.zeros((nx, nz), dt), img_pp=np.zeros((X, Z), dt),
@@ -143,10 +155,14 @@ class Oracle:
         if rec is not None:
             rx = np.ascontiguousarray(rec[0], dtype=np.float32)
             rz = np.ascontiguousarray(rec[1], dtype=np.float32)
-        f = self.lib.orc_rtm_f64 if fp64 else self.lib.orc_rtm_f32
         c = shot.cfg()
-        rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx), _ptr(rz),
-               *[_ptr(out[k], dt) for k in ("lap_pp", "lap_ps", "img_pp", "img_ps", "acc", "rec", "fields")])
+        outs = [_ptr(out[k], dt) for k in ("lap_pp", "lap_ps", "img_pp", "img_ps", "acc", "rec", "fields")]
+        if rho is not None:
+            rc = self.lib.orc_rtm_rho_f64(C.byref(c), _ptr(vp), _ptr(vs), _ptr(rho), _ptr(ax), _ptr(az), _ptr(src),
+                                          _ptr(rx), _ptr(rz), *outs)
+        else:
+            f = self.lib.orc_rtm_f64 if fp64 else self.lib.orc_rtm_f32
+            rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx), _ptr(rz), *outs)
         assert rc == 0
         return out
 

@@ -21,7 +21,7 @@ class ouc_config(C.Structure):
                 ("model_layout", C.c_int), ("strip_level", C.c_int), ("image_align", C.c_int),
                 ("strip_precision", C.c_int), ("compensated_image", C.c_int), ("gather_layout", C.c_int),
                 ("device", C.c_int), ("stream", C.c_void_p), ("max_batch", C.c_int), ("snapshot_every", C.c_int),
-                ("use_graphs", C.c_int)]
+                ("density", C.c_int), ("use_graphs", C.c_int)]
 
 
 class ouc_shot(C.Structure):

@@ -45,6 +45,7 @@ class Config:
     stream: int = 0
     max_batch: int = 1
     snapshot_every: int = 0     # 0: strips + reconstruction; K: source snapshots every K imaging levels
+    density: int = 0            # 1: variable density from rho (0: the reference's density-normalised equations)
     use_graphs: int = 1         # whole-shot time loops as CUDA graphs (captured once, replayed)
 
     def c(self):

@@ -126,6 +126,7 @@ StepArgs base_args(const ouc_ctx* c) {
     a.strip_slot = c->strip_slot;
     a.strip_prec = c->cfg.strip_precision;
     a.comp_image = c->cfg.compensated_image;
+    a.density = c->cfg.density;
     for (int k = 0; k < 3; ++k) a.comp[k] = c->comp[k];
     a.ring = c->ring;
     a.shots = c->d_desc;
@@ -225,6 +226,7 @@ int upload_desc(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_wavel
         d[b].off = (size_t)b * ctx->shot_stride;
         d[b].strip_slot = ctx->strip_slot;
         d[b].vp2 = ctx->vp2; d[b].vs2 = ctx->vs2; d[b].ax = ctx->ax; d[b].az = ctx->az;
+        d[b].bx = ctx->bx; d[b].bz = ctx->bz;
     }
     CK(cudaMemcpyAsync(ctx->d_desc, d.data(), n * sizeof(ShotDesc), cudaMemcpyHostToDevice, ctx->stream));
     return OUC_OK;
@@ -559,6 +561,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         cfg->strip_precision != OUC_PREC_BF16)
         return bad("strip_precision must be OUC_PREC_FP32, OUC_PREC_FP16 or OUC_PREC_BF16");
     if (cfg->compensated_image != 0 && cfg->compensated_image != 1) return bad("compensated_image must be 0 or 1");
+    if (cfg->density != 0 && cfg->density != 1) return bad("density must be 0 or 1");
     if (cfg->snapshot_every < 0 || cfg->snapshot_every > cfg->nt) return bad("snapshot_every must be in [0, nt]");
     ctx->N = N; ctx->L = L; ctx->nx = cfg->nx; ctx->nz = cfg->nz; ctx->nt = cfg->nt;
     ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
@@ -598,6 +601,35 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->vp_host = P_vp;
     std::vector<float> vp2((size_t)X * Z), vs2((size_t)X * Z);
     for (size_t k = 0; k < vp2.size(); ++k) { vp2[k] = P_vp[k] * P_vp[k]; vs2[k] = P_vs[k] * P_vs[k]; }
+    // variable density (no counterpart in the reference, whose equations are
+    // density-normalised, PS:373-378): moduli rho Vp^2, rho Vs^2 at the cells,
+    // buoyancy averaged onto the staggered Ux (i + 1/2) and Uz (j + 1/2) positions
+    std::vector<float> hbx, hbz;
+    if (cfg->density) {
+        if (!rho) return bad("density = 1 needs a density model");
+        std::vector<float> P_rho((size_t)X * Z);
+        if (cfg->model_layout == OUC_MODEL_PADDED) {
+            std::copy(rho, rho + (size_t)X * Z, P_rho.begin());
+        } else {
+            for (int i = 0; i < cfg->nx; ++i)
+                for (int j = 0; j < cfg->nz; ++j) P_rho[(size_t)(i + L) * Z + j + L] = rho[(size_t)i * cfg->nz + j];
+            pad_edges(P_rho, X, Z, L);
+        }
+        for (float v : P_rho)
+            if (!(v > 0) || !std::isfinite(v)) return bad("density must be positive and finite");
+        hbx.resize((size_t)X * Z);
+        hbz.resize((size_t)X * Z);
+        for (int i = 0; i < X; ++i)
+            for (int j = 0; j < Z; ++j) {
+                const size_t k = (size_t)i * Z + j;
+                vp2[k] = vp2[k] * P_rho[k];
+                vs2[k] = vs2[k] * P_rho[k];
+                const double b = 1.0 / P_rho[k];
+                const double bxn = i + 1 < X ? 1.0 / P_rho[k + Z] : b, bzn = j + 1 < Z ? 1.0 / P_rho[k + 1] : b;
+                hbx[k] = (float)(0.5 * (b + bxn));
+                hbz[k] = (float)(0.5 * (b + bzn));
+            }
+    }
 
     // device
     int ndev = 0;
@@ -646,7 +678,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         }
     }
 
-    const size_t model_bytes = 4 * ctx->fstride * sizeof(float);
+    const size_t model_bytes = 6 * ctx->fstride * sizeof(float);
     const size_t state_bytes = ctx->shot_stride * ctx->batch * sizeof(float);
     const size_t ng = (size_t)ctx->nt * X;
     const size_t ni = (size_t)ctx->nx * ctx->nz;
@@ -672,6 +704,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     for (int q = 0; q < 3; ++q) cudaMemsetAsync(ctx->d_stack[q], 0, ni * 8, ctx->stream);
     ctx->vp2 = ctx->field(ctx->model, 0); ctx->vs2 = ctx->field(ctx->model, 1);
     ctx->ax = ctx->field(ctx->model, 2); ctx->az = ctx->field(ctx->model, 3);
+    ctx->bx = ctx->field(ctx->model, 4); ctx->bz = ctx->field(ctx->model, 5);
     size_t k = 0;
     for (Side* s : {&ctx->src, &ctx->rcv}) {
         for (int q = 0; q < 4; ++q) s->now[q] = ctx->field(ctx->state, k++);
@@ -687,7 +720,8 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     configure_step_kernels(N);   // kernel attributes set before any graph capture
     int rc = OUC_OK;
     if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
-        (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data()))) {
+        (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data())) ||
+        (cfg->density && ((rc = upload_field(ctx, ctx->bx, hbx.data())) || (rc = upload_field(ctx, ctx->bz, hbz.data()))))) {
         ouc_destroy(ctx);
         return rc;
     }

@@ -53,9 +53,10 @@ struct ouc_ctx {
     std::vector<float> vp_host;  // padded Vp (for the mute's velocity)
 
     // device memory
-    float* model = nullptr;      // 4 fields: vp2 vs2 ax az
+    float* model = nullptr;      // 6 fields: vp2 vs2 ax az bx bz (moduli per unit density, or times rho)
     float* state = nullptr;      // batch shot blocks
     float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
+    float *bx = nullptr, *bz = nullptr;   // buoyancy at the Ux / Uz positions (cfg.density)
     Side src{}, rcv{};
     Side src0{}, rcv0{};         // leapfrog buffer assignment the whole-shot loops start from
     // CUDA graphs of whole-shot time loops (cfg.use_graphs), keyed by loop

@@ -213,11 +213,14 @@ struct Geo {
     const float* vs2;
     const float* ax;
     const float* az;
+    const float* bx;
+    const float* bz;
 };
 
 __device__ __forceinline__ Geo geo_of(const ShotDesc& d) {
     Geo gm;
     gm.X = d.X; gm.ring = d.ring; gm.vp2 = d.vp2; gm.vs2 = d.vs2; gm.ax = d.ax; gm.az = d.az;
+    gm.bx = d.bx; gm.bz = d.bz;
     return gm;
 }
 
@@ -659,10 +662,15 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
             // leapfrog brackets in the reference's order (PS:291-294); zero
             // memories outside the damping layers change no rounding
             const float4 nwx = make_float4(-wx[0].x, -wx[0].y, -wx[0].z, -wx[0].w);
-            const float4 spx = add4(sub4(sub4(add4(sub4(tx[0], oTx), dC), dE[0]), oC), oE);
-            const float4 spz = add4(sub4(sub4(add4(sub4(tz, oTz), dB[0]), dA), oB), oA);
-            const float4 ssx = add4(sub4(sub4(add4(sub4(wz, oWz), dC), dE[0]), oC), oE);
-            const float4 ssz = add4(sub4(sub4(add4(add4(nwx, oWx), dB[0]), dA), oB), oA);
+            float4 spx = add4(sub4(sub4(add4(sub4(tx[0], oTx), dC), dE[0]), oC), oE);
+            float4 spz = add4(sub4(sub4(add4(sub4(tz, oTz), dB[0]), dA), oB), oA);
+            float4 ssx = add4(sub4(sub4(add4(sub4(wz, oWz), dC), dE[0]), oC), oE);
+            float4 ssz = add4(sub4(sub4(add4(add4(nwx, oWx), dB[0]), dA), oB), oA);
+            if (p.density) {   // variable density: acceleration = buoyancy x stress divergence
+                const float4 bxv = ld4(gm.bx + g), bzv = ld4(gm.bz + g);
+                spx = mul4(spx, bxv); ssx = mul4(ssx, bxv);
+                spz = mul4(spz, bzv); ssz = mul4(ssz, bzv);
+            }
             const float4 npx = ld4(nowp[0] + g), npz = ld4(nowp[1] + g);
             const float4 nsx = ld4(nowp[2] + g), nsz = ld4(nowp[3] + g);
             const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);

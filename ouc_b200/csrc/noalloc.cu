@@ -157,6 +157,7 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     desc.off = 0;
     desc.strip_slot = 0;
     desc.vp2 = field(0); desc.vs2 = field(1); desc.ax = field(2); desc.az = field(3);
+    desc.bx = nullptr; desc.bz = nullptr;   // density-normalised equations only
     if (cudaMemcpyAsync(d_desc, &desc, sizeof(desc), cudaMemcpyHostToDevice, stream) != cudaSuccess) return OUC_ECUDA;
 
     StepArgs a;

@@ -92,10 +92,12 @@ struct ShotDesc {
     Ring ring;                     // boundary ring of this grid
     size_t off;                    // offset (floats) of this shot's fields from shot 0's
     size_t strip_slot;             // floats per strip slot
-    const float* vp2;              // model views of this grid, cell (0, 0)
-    const float* vs2;
+    const float* vp2;              // model views of this grid, cell (0, 0): the moduli
+    const float* vs2;              // (rho) Vp^2 and (rho) Vs^2, damping x and z,
     const float* ax;
     const float* az;
+    const float* bx;               // and with StepArgs.density the buoyancy at the Ux
+    const float* bz;               // and Uz positions
 };
 
 struct StepArgs {
@@ -108,6 +110,7 @@ struct StepArgs {
     int img_past;                     // kRec: correlate with level t+2 (reference alignment)
     int strip_prec;                   // StripPrec of the strips
     int comp_image;                   // kRec: compensated (Kahan) imaging sums, comp[] below
+    int density;                      // variable density: scale the U-stage by the buoyancy
     float a[6];                       // stencil weights a_1..a_N
     float dx, dz, dt, dt2;
     float rdx, rdz;                   // RN(1/dx), RN(1/dz)

@@ -34,7 +34,7 @@ using namespace host;
         if (e_ != cudaSuccess) return host::cuda_fail(ctx, e_, #call);     \
     } while (0)
 
-constexpr int kModelFields = 4;   // vp2 vs2 ax az per batch slot
+constexpr int kModelFields = 6;   // vp2 vs2 ax az bx bz per batch slot
 
 float* slot_field(const ouc_ctx* c, int b, int k) {
     return c->sv_model + ((size_t)b * kModelFields + k) * c->fstride + (size_t)kGX * c->pitch + kZOFF;
@@ -82,8 +82,10 @@ int upload_batch(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture*
     for (int b = 0; b < n; ++b) {
         const Window w{ap[b].x0, ap[b].x1 - ap[b].x0 + 2 * L};
         // model window: rows [x0, x0 + X) of the padded model, guard columns included
-        for (int k = 0; k < 2; ++k) {
-            const float* src = (k == 0 ? ctx->vp2 : ctx->vs2) - kZOFF + (size_t)w.x0 * pitch;
+        const float* window_src[kModelFields] = {ctx->vp2, ctx->vs2, nullptr, nullptr, ctx->bx, ctx->bz};
+        for (int k = 0; k < kModelFields; ++k) {
+            if (!window_src[k] || (k >= 4 && !ctx->cfg.density)) continue;
+            const float* src = window_src[k] - kZOFF + (size_t)w.x0 * pitch;
             CKS(cudaMemcpyAsync(slot_field(ctx, b, k) - kZOFF, src, (size_t)w.X * pitch * sizeof(float),
                                 cudaMemcpyDeviceToDevice, ctx->stream));
         }
@@ -120,6 +122,7 @@ int upload_batch(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture*
         s.strip_slot = ctx->strip_slot;
         s.vp2 = slot_field(ctx, b, 0); s.vs2 = slot_field(ctx, b, 1);
         s.ax = slot_field(ctx, b, 2); s.az = slot_field(ctx, b, 3);
+        s.bx = slot_field(ctx, b, 4); s.bz = slot_field(ctx, b, 5);
     }
     CKS(cudaMemcpyAsync(ctx->d_desc, d.data(), n * sizeof(ShotDesc), cudaMemcpyHostToDevice, ctx->stream));
     return OUC_OK;
