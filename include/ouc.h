@@ -94,6 +94,8 @@ typedef struct ouc_config {
                                staggered Ux/Uz positions); 0: the reference's
                                density-normalised equations, rho ignored (no
                                counterpart in the reference for 1)             */
+    int gradient;           /* 1: RTM shots also accumulate the FWI gradient
+                               (ouc_gradient; strip form, density = 0)        */
     int use_graphs;         /* 1: capture each whole-shot time loop (one launch
                                per stage and step) as a CUDA graph on first use
                                and replay it for later shots and batches        */
@@ -182,6 +184,23 @@ int ouc_rtm_batch_dev(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const flo
  * Any output may be NULL; reset != 0 clears the stack after reading. */
 int ouc_stack(ouc_ctx* ctx, double* stack_pp, double* stack_ps, double* illum, int reset);
 int ouc_stack_dev(ouc_ctx* ctx, const double** d_pp, const double** d_ps, const double** d_illum);
+
+/* FWI gradient (cfg.gradient = 1; the step after imaging: the formula of the
+ * reference's gradfun/caculate_Grad, PS:1518-1633, which its main() never
+ * calls).  At every back-step of an RTM shot, with U_s = P + S the source
+ * displacement at the level the imaging condition correlates there and the
+ * receiver's stress fields (theta, omega, Q, PS:373-378) recomputed from its
+ * displacement after the step, on the interior cells at least N from the
+ * absorbing layers:
+ *   G_vp -= 2 rho Vp (dUx/dx + dUz/dz) theta_r
+ *   G_vs -= 2 rho Vs (omega_r (dUx/dz - dUz/dx) + Qzx_r dUz/dx + Qzz_r dUz/dz
+ *                     + Qxz_r dUx/dz + Qxx_r dUx/dx)
+ *   illum += Ux_s^2 + Uz_s^2
+ * (rho from ouc_create's rho model, 1 without one; the reference's dUx/dz
+ * stencil typo, PS:1556, is not reproduced).  Shots add into FP64 stacks in
+ * order; ouc_gradient reads them (nx*nz each, any may be NULL), reset != 0
+ * clears them. */
+int ouc_gradient(ouc_ctx* ctx, double* g_vp, double* g_vs, double* illum, int reset);
 
 /* Step-level interface: one RTM shot advanced one reference time step per
  * call, for comparing against the reference's kernels step by step.  The

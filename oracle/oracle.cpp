@@ -308,6 +308,10 @@ struct Engine {
     T a[8];
     T dx, dz, dt;
     Model<T> m;
+    // FWI gradient (rtm with grad_out): rho of the formula (null: 1) and the
+    // output [3][X][Z]: gradient w.r.t. Vp, w.r.t. Vs, source illumination
+    const float* grad_rho = nullptr;
+    T* grad_out = nullptr;
 
     void setup(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
                const float* rho = nullptr) {
@@ -352,6 +356,51 @@ struct Engine {
         for (int i = N; i < X - N; ++i)
             for (int j = N; j < Z - N; ++j) u_cell<T>(w, m, a, N, dx, dz, dt, i, j);
     }
+    // FWI gradient at one back-step (the formula of the reference's unused
+    // gradfun, PS:1518-1575): the source displacement U_s = P + S at the level
+    // the imaging condition correlates, its four staggered derivatives, the
+    // receiver's stress fields recomputed from its displacement U_r after the
+    // back-step (PS:373-378; no damping memories on these cells):
+    //   G_vp -= 2 rho Vp (dUx/dx + dUz/dz) theta_r
+    //   G_vs -= 2 rho Vs (omega_r (dUx/dz - dUz/dx) + Qzx_r dUz/dx + Qzz_r dUz/dz
+    //                     + Qxz_r dUx/dz + Qxx_r dUx/dx)
+    //   S    += Ux_s^2 + Uz_s^2
+    // on [L+N, X-L-N) x [L+N, Z-L-N), where every stencil reads interior
+    // cells only.  The reference's dUx/dz stencil has a typo in its fourth term
+    // (j - 6 for j - 3, PS:1556); the correct stencil is used.
+    void gradient(const Field<T>& spx, const Field<T>& spz, const Field<T>& ssx, const Field<T>& ssz,
+                  const Wave<T>& wr) {
+        const size_t C = (size_t)X * Z;
+        std::vector<T> usx(C), usz(C), urx(C), urz(C);
+#pragma omp parallel for schedule(static)
+        for (int i = L; i < X - L; ++i)
+            for (int j = L; j < Z - L; ++j) {
+                const size_t c = (size_t)i * Z + j;
+                usx[c] = spx.v[c] + ssx.v[c]; usz[c] = spz.v[c] + ssz.v[c];
+                urx[c] = wr.pnx.v[c] + wr.snx.v[c]; urz[c] = wr.pnz.v[c] + wr.snz.v[c];
+            }
+        T* gvp = grad_out;
+        T* gvs = grad_out + C;
+        T* sss = grad_out + 2 * C;
+#pragma omp parallel for schedule(static)
+        for (int i = L + N; i < X - L - N; ++i)
+            for (int j = L + N; j < Z - L - N; ++j) {
+                const size_t c = (size_t)i * Z + j;
+                const ptrdiff_t sZ = Z;
+                const T sxx = dminus(usx.data() + c, sZ, a, N, dx), szz = dminus(usz.data() + c, (ptrdiff_t)1, a, N, dz);
+                const T szx = dplus(usz.data() + c, sZ, a, N, dx), sxz = dplus(usx.data() + c, (ptrdiff_t)1, a, N, dz);
+                const T rxx = dminus(urx.data() + c, sZ, a, N, dx), rzz = dminus(urz.data() + c, (ptrdiff_t)1, a, N, dz);
+                const T rzx = dplus(urz.data() + c, sZ, a, N, dx), rxz = dplus(urx.data() + c, (ptrdiff_t)1, a, N, dz);
+                const T vp = m.vp.v[c], vs = m.vs.v[c], vp2 = vp * vp, vs2 = vs * vs;
+                const T rho = grad_rho ? (T)grad_rho[c] : T(1);
+                const T th = vp2 * (rxx + rzz), om = vs2 * (rxz - rzx);
+                const T qzx = vs2 * rzx, qzz = vs2 * rzz, qxz = vs2 * rxz, qxx = vs2 * rxx;
+                gvp[c] -= 2 * rho * vp * ((sxx + szz) * th);
+                gvs[c] -= 2 * rho * vs * (om * (sxz - szx) + qzx * szx + qzz * szz + qxz * sxz + qxx * sxx);
+                sss[c] += usx[c] * usx[c] + usz[c] * usz[c];
+            }
+    }
+
     // Receiver extraction.  The reference's test is an assignment (PS:307),
     // so every thread races to store Vx[i][Z_receive]; the deterministic
     // reading kept here is the post-update value, i.e. the one the
@@ -468,6 +517,11 @@ struct Engine {
             // corr_v (PS:2361): zero-lag PP / PS / illumination on the interior
             const Field<T>& spx = (cfg.image_align == 0 || t == nt - 1) ? prev[0] : r.pnx;
             const Field<T>& spz = (cfg.image_align == 0 || t == nt - 1) ? prev[1] : r.pnz;
+            if (grad_out) {
+                const Field<T>& ssx = (cfg.image_align == 0 || t == nt - 1) ? prev[2] : r.snx;
+                const Field<T>& ssz = (cfg.image_align == 0 || t == nt - 1) ? prev[3] : r.snz;
+                gradient(spx, spz, ssx, ssz, wr);
+            }
 #pragma omp parallel for schedule(static)
             for (int i = L; i < X - L; ++i)
                 for (int j = L; j < Z - L; ++j) {
@@ -559,6 +613,32 @@ int orc_rtm_f64(const orc_cfg* c, const float* vp, const float* vs, const float*
     Engine<double> e;
     e.setup(c, vp, vs, ax, az);
     e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, raw_pp, raw_ps, acc, rec_out, fields_out);
+    return 0;
+}
+
+// RTM with the FWI gradient (see Engine::gradient): grad [3][X][Z] receives
+// the gradient w.r.t. Vp, w.r.t. Vs and the source illumination of one shot;
+// rho (padded, may be NULL for 1) enters the gradient formula only.
+int orc_rtm_grad_f64(const orc_cfg* c, const float* vp, const float* vs, const float* rho, const float* ax,
+                     const float* az, const float* src, const float* rec_x, const float* rec_z, double* lap_pp,
+                     double* lap_ps, double* grad) {
+    Engine<double> e;
+    e.setup(c, vp, vs, ax, az);
+    e.grad_rho = rho;
+    std::fill(grad, grad + 3 * (size_t)c->X * c->Z, 0.0);
+    e.grad_out = grad;
+    e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, nullptr, nullptr, nullptr, nullptr, nullptr);
+    return 0;
+}
+int orc_rtm_grad_f32(const orc_cfg* c, const float* vp, const float* vs, const float* rho, const float* ax,
+                     const float* az, const float* src, const float* rec_x, const float* rec_z, float* lap_pp,
+                     float* lap_ps, float* grad) {
+    Engine<float> e;
+    e.setup(c, vp, vs, ax, az);
+    e.grad_rho = rho;
+    std::fill(grad, grad + 3 * (size_t)c->X * c->Z, 0.f);
+    e.grad_out = grad;
+    e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, nullptr, nullptr, nullptr, nullptr, nullptr);
     return 0;
 }
 

@@ -102,6 +102,10 @@ class Oracle:
         self.lib.orc_rtm_rho_f64.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _dp, _dp, _dp,
                                              _dp, _dp, _dp, _dp]
         self.lib.orc_rtm_rho_f64.restype = C.c_int
+        for name, t in (("orc_rtm_grad_f32", _fp), ("orc_rtm_grad_f64", _dp)):
+            f = getattr(self.lib, name)
+            f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, t, t, t]
+            f.restype = C.c_int
         self.lib.orc_pad_model.argtypes = [_fp, C.c_int, C.c_int, C.c_int]
         self.lib.orc_cpml_profile.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_double, _fp, _fp]
         self.lib.orc_num_threads.restype = C.c_int
@@ -165,6 +169,29 @@ class Oracle:
             rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx), _ptr(rz), *outs)
         assert rc == 0
         return out
+
+
+def _none_or(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def rtm_gradient(orc, shot, vp, vs, ax, az, src, rec=None, rho=None, fp64=True):
+    """RTM with the FWI gradient: (lap_pp, lap_ps, grad [3][X][Z]) -- gradient
+    w.r.t. Vp, w.r.t. Vs and the source illumination of one shot."""
+    dt = np.float64 if fp64 else np.float32
+    X, Z, L = shot.X, shot.Z, shot.L
+    lpp = np.zeros((X - 2 * L, Z - 2 * L), dt)
+    lps = np.zeros_like(lpp)
+    grad = np.zeros((3, X, Z), dt)
+    rx = rz = None
+    if rec is not None:
+        rx, rz = _none_or(rec[0]), _none_or(rec[1])
+    f = orc.lib.orc_rtm_grad_f64 if fp64 else orc.lib.orc_rtm_grad_f32
+    c = shot.cfg()
+    rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(_none_or(rho)), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx), _ptr(rz),
+           _ptr(lpp, dt), _ptr(lps, dt), _ptr(grad, dt))
+    assert rc == 0
+    return lpp, lps, grad
 
 
 class RefBuild:

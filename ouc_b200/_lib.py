@@ -21,7 +21,7 @@ class ouc_config(C.Structure):
                 ("model_layout", C.c_int), ("strip_level", C.c_int), ("image_align", C.c_int),
                 ("strip_precision", C.c_int), ("compensated_image", C.c_int), ("gather_layout", C.c_int),
                 ("device", C.c_int), ("stream", C.c_void_p), ("max_batch", C.c_int), ("snapshot_every", C.c_int),
-                ("density", C.c_int), ("use_graphs", C.c_int)]
+                ("density", C.c_int), ("gradient", C.c_int), ("use_graphs", C.c_int)]
 
 
 class ouc_shot(C.Structure):
@@ -71,6 +71,7 @@ SIGNATURES = {
     "ouc_set_run_batch": (C.c_int, [_vp, C.c_int]),
     "ouc_forward_noalloc": (C.c_int, [C.POINTER(ouc_config), C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
     "ouc_stack": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
+    "ouc_gradient": (C.c_int, [_vp, _dp, _dp, _dp, C.c_int]),
     "ouc_stack_dev": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
     "ouc_step_begin": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp]),
     "ouc_step_forward": (C.c_int, [_vp, C.c_int]),

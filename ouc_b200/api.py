@@ -46,6 +46,7 @@ class Config:
     max_batch: int = 1
     snapshot_every: int = 0     # 0: strips + reconstruction; K: source snapshots every K imaging levels
     density: int = 0            # 1: variable density from rho (0: the reference's density-normalised equations)
+    gradient: int = 0           # 1: RTM shots also accumulate the FWI gradient (Context.gradient)
     use_graphs: int = 1         # whole-shot time loops as CUDA graphs (captured once, replayed)
 
     def c(self):
@@ -325,6 +326,16 @@ class Context:
         p = [C.c_void_p(), C.c_void_p(), C.c_void_p()]
         check(lib().ouc_stack_dev(self._h, C.byref(p[0]), C.byref(p[1]), C.byref(p[2])), self._h)
         return tuple(q.value for q in p)
+
+    def gradient(self, reset=False):
+        """FP64 stacks of the FWI gradient w.r.t. Vp and Vs and of the source
+        illumination, each nx x nz (cfg.gradient = 1)."""
+        n = (self.cfg.nx, self.cfg.nz)
+        gp, gs, il = np.zeros(n), np.zeros(n), np.zeros(n)
+        dp = C.POINTER(C.c_double)
+        check(lib().ouc_gradient(self._h, gp.ctypes.data_as(dp), gs.ctypes.data_as(dp), il.ctypes.data_as(dp),
+                                 int(reset)), self._h)
+        return gp, gs, il
 
     def stack(self, reset=False):
         n = (self.cfg.nx, self.cfg.nz)

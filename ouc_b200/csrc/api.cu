@@ -169,6 +169,22 @@ int ensure_strips(ouc_ctx* ctx) {
     return OUC_OK;
 }
 
+int ensure_grad(ouc_ctx* ctx) {
+    if (ctx->grad) return OUC_OK;
+    const size_t bytes = (size_t)ctx->batch * 3 * ctx->fstride * sizeof(float);
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    bool ok = cudaMalloc(&ctx->grad, bytes) == cudaSuccess;
+    for (int k = 0; k < 3 && ok; ++k) ok = cudaMalloc(&ctx->d_gstack[k], ni * 8) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        return fail(ctx, OUC_ENOMEM, "cannot allocate the gradient accumulators");
+    }
+    for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->d_gstack[k], 0, ni * 8, ctx->stream));
+    CK(cudaMemsetAsync(ctx->grad, 0, bytes, ctx->stream));   // guard cells stay zero
+    ctx->bytes += bytes + 3 * ni * 8;
+    return OUC_OK;
+}
+
 int ensure_snaps(ouc_ctx* ctx) {
     if (ctx->snaps) return OUC_OK;
     const int prec = ctx->cfg.strip_precision;
@@ -385,8 +401,28 @@ int rec_step(ouc_ctx* ctx, StepArgs& as, Side& s, const Side& r, int n, int t, b
 
 // Backward loop (PS:2313-2364) and imaging of n shots; the source side
 // holds the forward's last two levels on entry.
+// FWI gradient of back-step t, launched between the receiver step and the
+// reconstruction: the source level the imaging condition correlates at this
+// step (the forward's last level at t = nt-1), the receiver after the step.
+void grad_step(ouc_ctx* ctx, const Side& s, const Side& r, int n, int t) {
+    GradArgs g;
+    memset(&g, 0, sizeof(g));
+    g.X = ctx->X; g.Z = ctx->Z; g.pitch = ctx->pitch; g.L = ctx->L; g.N = ctx->N;
+    g.nshots = n;
+    for (int k = 0; k < 6; ++k) g.a[k] = ctx->a[k];
+    g.dx = ctx->cfg.dx; g.dz = ctx->cfg.dz;
+    const bool past = t < ctx->nt - 1 && ctx->cfg.image_align == OUC_IMAGE_REFERENCE;
+    for (int k = 0; k < 4; ++k) { g.src[k] = past ? s.past[k] : s.now[k]; g.rcv[k] = r.now[k]; }
+    g.shot_stride = ctx->shot_stride;
+    g.vp = ctx->vpv; g.vs = ctx->vsv; g.rho = ctx->rhov;
+    for (int k = 0; k < 3; ++k) g.g[k] = ctx->grad + (size_t)k * ctx->fstride + (size_t)kGX * ctx->pitch + kZOFF;
+    g.grad_stride = 3 * ctx->fstride;
+    launch_grad(g, ctx->stream);
+    ctx->timing.kernel_launches += 1;
+}
+
 int run_backward(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
-    const int key[6] = {1, n, exact_strips, theta_src, 0, 0};
+    const int key[6] = {1, n, exact_strips, theta_src, 0, ctx->cfg.gradient};
     return with_graph(ctx, key, [&]() { return run_backward_loop(ctx, n, exact_strips, theta_src); });
 }
 
@@ -395,10 +431,12 @@ int run_backward_loop(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
     Side r = ctx->rcv0;
     int rc = zero_side(ctx, n, 1, true);
     if (rc) return rc;
+    if (ctx->cfg.gradient) CK(cudaMemsetAsync(ctx->grad, 0, (size_t)n * 3 * ctx->fstride * sizeof(float), ctx->stream));
     StepArgs ar = rcv_args(ctx);
     StepArgs as = rec_args(ctx);
     for (int t = ctx->nt - 1; t >= 0; --t) {
         if ((rc = rcv_step(ctx, ar, r, n, t))) return rc;
+        if (ctx->cfg.gradient) grad_step(ctx, s, r, n, t);
         if ((rc = rec_step(ctx, as, s, r, n, t, exact_strips, theta_src))) return rc;
     }
     CK(cudaGetLastError());
@@ -562,6 +600,9 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         return bad("strip_precision must be OUC_PREC_FP32, OUC_PREC_FP16 or OUC_PREC_BF16");
     if (cfg->compensated_image != 0 && cfg->compensated_image != 1) return bad("compensated_image must be 0 or 1");
     if (cfg->density != 0 && cfg->density != 1) return bad("density must be 0 or 1");
+    if (cfg->gradient != 0 && cfg->gradient != 1) return bad("gradient must be 0 or 1");
+    if (cfg->gradient && (cfg->density || cfg->snapshot_every > 0))
+        return bad("the FWI gradient runs with the density-normalised equations and the strip form");
     if (cfg->snapshot_every < 0 || cfg->snapshot_every > cfg->nt) return bad("snapshot_every must be in [0, nt]");
     ctx->N = N; ctx->L = L; ctx->nx = cfg->nx; ctx->nz = cfg->nz; ctx->nt = cfg->nt;
     ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
@@ -604,10 +645,10 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     // variable density (no counterpart in the reference, whose equations are
     // density-normalised, PS:373-378): moduli rho Vp^2, rho Vs^2 at the cells,
     // buoyancy averaged onto the staggered Ux (i + 1/2) and Uz (j + 1/2) positions
-    std::vector<float> hbx, hbz;
-    if (cfg->density) {
-        if (!rho) return bad("density = 1 needs a density model");
-        std::vector<float> P_rho((size_t)X * Z);
+    std::vector<float> hbx, hbz, P_rho;
+    if (cfg->density && !rho) return bad("density = 1 needs a density model");
+    if (rho) {   // padded density: the variable-density equations and the FWI gradient formula
+        P_rho.resize((size_t)X * Z);
         if (cfg->model_layout == OUC_MODEL_PADDED) {
             std::copy(rho, rho + (size_t)X * Z, P_rho.begin());
         } else {
@@ -617,6 +658,8 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         }
         for (float v : P_rho)
             if (!(v > 0) || !std::isfinite(v)) return bad("density must be positive and finite");
+    }
+    if (cfg->density) {
         hbx.resize((size_t)X * Z);
         hbz.resize((size_t)X * Z);
         for (int i = 0; i < X; ++i)
@@ -678,7 +721,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         }
     }
 
-    const size_t model_bytes = 6 * ctx->fstride * sizeof(float);
+    const size_t model_bytes = 9 * ctx->fstride * sizeof(float);
     const size_t state_bytes = ctx->shot_stride * ctx->batch * sizeof(float);
     const size_t ng = (size_t)ctx->nt * X;
     const size_t ni = (size_t)ctx->nx * ctx->nz;
@@ -705,6 +748,8 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->vp2 = ctx->field(ctx->model, 0); ctx->vs2 = ctx->field(ctx->model, 1);
     ctx->ax = ctx->field(ctx->model, 2); ctx->az = ctx->field(ctx->model, 3);
     ctx->bx = ctx->field(ctx->model, 4); ctx->bz = ctx->field(ctx->model, 5);
+    ctx->vpv = ctx->field(ctx->model, 6); ctx->vsv = ctx->field(ctx->model, 7);
+    ctx->rhov = P_rho.empty() ? nullptr : ctx->field(ctx->model, 8);
     size_t k = 0;
     for (Side* s : {&ctx->src, &ctx->rcv}) {
         for (int q = 0; q < 4; ++q) s->now[q] = ctx->field(ctx->state, k++);
@@ -721,7 +766,9 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     int rc = OUC_OK;
     if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
         (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data())) ||
-        (cfg->density && ((rc = upload_field(ctx, ctx->bx, hbx.data())) || (rc = upload_field(ctx, ctx->bz, hbz.data()))))) {
+        (cfg->density && ((rc = upload_field(ctx, ctx->bx, hbx.data())) || (rc = upload_field(ctx, ctx->bz, hbz.data())))) ||
+        (rc = upload_field(ctx, ctx->vpv, P_vp.data())) || (rc = upload_field(ctx, ctx->vsv, P_vs.data())) ||
+        (ctx->rhov && (rc = upload_field(ctx, ctx->rhov, P_rho.data())))) {
         ouc_destroy(ctx);
         return rc;
     }
@@ -740,6 +787,8 @@ int ouc_destroy(ouc_ctx* ctx) {
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
     cudaFree(ctx->l_in); cudaFree(ctx->l_out); cudaFree(ctx->l_truth); cudaFree(ctx->l_scale); cudaFree(ctx->l_tmp); cudaFree(ctx->sv_model);
+    cudaFree(ctx->grad);
+    for (auto* p : ctx->d_gstack) cudaFree(p);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -843,6 +892,17 @@ static int rtm_group(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     if ((rc = finalize(ctx, n))) return rc;
+    if (ctx->cfg.gradient) {
+        GradStackArgs gs;
+        gs.X = ctx->X; gs.Z = ctx->Z; gs.pitch = ctx->pitch; gs.L = ctx->L; gs.nshots = n;
+        for (int k = 0; k < 3; ++k) {
+            gs.g[k] = ctx->grad + (size_t)k * ctx->fstride + (size_t)kGX * ctx->pitch + kZOFF;
+            gs.stack[k] = ctx->d_gstack[k];
+        }
+        gs.grad_stride = 3 * ctx->fstride;
+        launch_grad_stack(gs, ctx->stream);
+        ctx->timing.kernel_launches += 1;
+    }
     const size_t ni = (size_t)ctx->nx * ctx->nz;
     const cudaMemcpyKind kind = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     for (int b = 0; b < n; ++b) {
@@ -870,6 +930,7 @@ static int rtm_batch_impl(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const
     cudaSetDevice(ctx->device);
     ctx->step_phase = ouc_ctx::kIdle;   // whole-shot calls overwrite any stepped state
     if ((rc = ctx->cfg.snapshot_every > 0 ? ensure_snaps(ctx) : ensure_strips(ctx))) return rc;
+    if (ctx->cfg.gradient && (rc = ensure_grad(ctx))) return rc;
     ctx->timing = ouc_timing{};
     const float* d_w = wavelet;
     if (host) {
@@ -915,6 +976,21 @@ int ouc_stack(ouc_ctx* ctx, double* pp, double* ps, double* illum, int reset) {
         if (outs[k]) CK(cudaMemcpyAsync(outs[k], ctx->d_stack[k], ni * 8, cudaMemcpyDeviceToHost, ctx->stream));
     if (reset)
         for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->d_stack[k], 0, ni * 8, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OUC_OK;
+}
+
+int ouc_gradient(ouc_ctx* ctx, double* g_vp, double* g_vs, double* illum, int reset) {
+    if (!ctx) return OUC_EINVAL;
+    if (!ctx->cfg.gradient) return fail(ctx, OUC_ESTATE, "the context was created without gradient = 1");
+    if (!ctx->grad) return fail(ctx, OUC_ESTATE, "no RTM shot has run yet");
+    cudaSetDevice(ctx->device);
+    const size_t ni = (size_t)ctx->nx * ctx->nz;
+    double* out[3] = {g_vp, g_vs, illum};
+    for (int k = 0; k < 3; ++k)
+        if (out[k]) CK(cudaMemcpyAsync(out[k], ctx->d_gstack[k], ni * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (reset)
+        for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->d_gstack[k], 0, ni * 8, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return OUC_OK;
 }

@@ -53,10 +53,14 @@ struct ouc_ctx {
     std::vector<float> vp_host;  // padded Vp (for the mute's velocity)
 
     // device memory
-    float* model = nullptr;      // 6 fields: vp2 vs2 ax az bx bz (moduli per unit density, or times rho)
+    float* model = nullptr;      // 9 fields: vp2 vs2 ax az bx bz (moduli per unit density, or times rho), vp vs rho
     float* state = nullptr;      // batch shot blocks
     float *vp2 = nullptr, *vs2 = nullptr, *ax = nullptr, *az = nullptr;
     float *bx = nullptr, *bz = nullptr;   // buoyancy at the Ux / Uz positions (cfg.density)
+    float *vpv = nullptr, *vsv = nullptr, *rhov = nullptr;   // Vp, Vs, rho (null without a rho model)
+    // FWI gradient (cfg.gradient): per-shot accumulators [batch][3] and FP64 stacks
+    float* grad = nullptr;
+    double* d_gstack[3] = {nullptr, nullptr, nullptr};
     Side src{}, rcv{};
     Side src0{}, rcv0{};         // leapfrog buffer assignment the whole-shot loops start from
     // CUDA graphs of whole-shot time loops (cfg.use_graphs), keyed by loop

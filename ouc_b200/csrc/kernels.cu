@@ -337,6 +337,124 @@ void launch_transpose(const float* in, float* out, int rows, int cols, cudaStrea
 }
 
 // Gather nf pitched fields into a dense [nf][X][Z] buffer.
+// FWI gradient of one back-step (the formula of the reference's unused
+// gradfun, PS:1518-1575), for every shot of the launch (blockIdx.y):
+//   G_vp -= 2 rho Vp (dUx/dx + dUz/dz) theta_r
+//   G_vs -= 2 rho Vs (omega_r (dUx/dz - dUz/dx) + Qzx_r dUz/dx + Qzz_r dUz/dz + Qxz_r dUx/dz + Qxx_r dUx/dx)
+//   S    += Ux_s^2 + Uz_s^2
+// with U_s = P + S of the source at the imaged level, its staggered
+// derivatives (dUx/dx = D-x, dUz/dz = D-z, dUz/dx = D+x, dUx/dz = D+z), and
+// the receiver's stress fields from U_r = P + S after the back-step
+// (PS:373-378 without damping memories), on [L+N, X-L-N) x [L+N, Z-L-N):
+// every stencil reads interior cells only.  A CTA stages the four U fields
+// of a 16 x 64 tile with an N-row and 8-column halo in shared memory.
+template <int N>
+__global__ void __launch_bounds__(256) k_grad(const GradArgs a) {
+    constexpr int TR = 16, TC = 64, HC = 8, BR = TR + 2 * N, BC = TC + 2 * HC;
+    __shared__ float4 sbox4[4 * BR * BC / 4];
+    float* box = reinterpret_cast<float*>(sbox4);
+    const int b = blockIdx.y;
+    const int tiles_c = (a.Z + TC - 1) / TC;
+    const int x0 = (blockIdx.x / tiles_c) * TR, z0 = (blockIdx.x % tiles_c) * TC;
+    const size_t off = (size_t)b * a.shot_stride;
+    for (int k = threadIdx.x; k < BR * (BC / 4); k += blockDim.x) {
+        const int r = k / (BC / 4), c4 = k - r * (BC / 4);
+        const ptrdiff_t g = (ptrdiff_t)(x0 - N + r) * a.pitch + (z0 - HC + 4 * c4);
+        const float4 spx = *reinterpret_cast<const float4*>(a.src[0] + off + g);
+        const float4 spz = *reinterpret_cast<const float4*>(a.src[1] + off + g);
+        const float4 ssx = *reinterpret_cast<const float4*>(a.src[2] + off + g);
+        const float4 ssz = *reinterpret_cast<const float4*>(a.src[3] + off + g);
+        const float4 rpx = *reinterpret_cast<const float4*>(a.rcv[0] + off + g);
+        const float4 rpz = *reinterpret_cast<const float4*>(a.rcv[1] + off + g);
+        const float4 rsx = *reinterpret_cast<const float4*>(a.rcv[2] + off + g);
+        const float4 rsz = *reinterpret_cast<const float4*>(a.rcv[3] + off + g);
+        float4* o = sbox4 + r * (BC / 4) + c4;
+        o[0 * BR * BC / 4] = make_float4(spx.x + ssx.x, spx.y + ssx.y, spx.z + ssx.z, spx.w + ssx.w);
+        o[1 * BR * BC / 4] = make_float4(spz.x + ssz.x, spz.y + ssz.y, spz.z + ssz.z, spz.w + ssz.w);
+        o[2 * BR * BC / 4] = make_float4(rpx.x + rsx.x, rpx.y + rsx.y, rpx.z + rsx.z, rpx.w + rsx.w);
+        o[3 * BR * BC / 4] = make_float4(rpz.x + rsz.x, rpz.y + rsz.y, rpz.z + rsz.z, rpz.w + rsz.w);
+    }
+    __syncthreads();
+    const float* usx = box;
+    const float* usz = box + BR * BC;
+    const float* urx = box + 2 * BR * BC;
+    const float* urz = box + 3 * BR * BC;
+    auto at = [&](const float* f, int r, int c) { return f[(r + N) * BC + (c + HC)]; };
+    // staggered derivatives at tile cell (r, c), PS:224-279 stencil forms
+    auto dmx = [&](const float* f, int r, int c) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 1; k <= N; ++k) acc = fmaf(a.a[k - 1], at(f, r + k - 1, c) - at(f, r - k, c), acc);
+        return acc / a.dx;
+    };
+    auto dpx = [&](const float* f, int r, int c) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 1; k <= N; ++k) acc = fmaf(a.a[k - 1], at(f, r + k, c) - at(f, r - k + 1, c), acc);
+        return acc / a.dx;
+    };
+    auto dmz = [&](const float* f, int r, int c) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 1; k <= N; ++k) acc = fmaf(a.a[k - 1], at(f, r, c + k - 1) - at(f, r, c - k), acc);
+        return acc / a.dz;
+    };
+    auto dpz = [&](const float* f, int r, int c) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 1; k <= N; ++k) acc = fmaf(a.a[k - 1], at(f, r, c + k) - at(f, r, c - k + 1), acc);
+        return acc / a.dz;
+    };
+    const int r = threadIdx.x / (TC / 4), c0 = 4 * (threadIdx.x % (TC / 4));
+    const int i = x0 + r;
+    if (r >= TR || i < a.L + N || i >= a.X - a.L - N) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int c = c0 + q, j = z0 + c;
+        if (j < a.L + N || j >= a.Z - a.L - N) continue;
+        const float sxx = dmx(usx, r, c), szz = dmz(usz, r, c), szx = dpx(usz, r, c), sxz = dpz(usx, r, c);
+        const float rxx = dmx(urx, r, c), rzz = dmz(urz, r, c), rzx = dpx(urz, r, c), rxz = dpz(urx, r, c);
+        const ptrdiff_t g = (ptrdiff_t)i * a.pitch + j;
+        const float vp = a.vp[g], vs = a.vs[g], vp2 = vp * vp, vs2 = vs * vs;
+        const float rho = a.rho ? a.rho[g] : 1.f;
+        const float th = vp2 * (rxx + rzz), om = vs2 * (rxz - rzx);
+        const float s_vs = om * (sxz - szx) + vs2 * rzx * szx + vs2 * rzz * szz + vs2 * rxz * sxz + vs2 * rxx * sxx;
+        const size_t og = (size_t)b * a.grad_stride + g;
+        a.g[0][og] -= 2.f * rho * vp * ((sxx + szz) * th);
+        a.g[1][og] -= 2.f * rho * vs * s_vs;
+        const float ux = at(usx, r, c), uz = at(usz, r, c);
+        a.g[2][og] += ux * ux + uz * uz;
+    }
+}
+
+void launch_grad(const GradArgs& a, cudaStream_t s) {
+    // tile rows only up to the last gradient row X-L-N-1: the staged rows then
+    // end below X-L+14, inside the fields' 16 guard rows
+    const int tiles = ((a.X - a.L - a.N + 15) / 16) * ((a.Z + 63) / 64);
+    const dim3 grid(tiles, a.nshots);
+    if (a.N == 2) k_grad<2><<<grid, 256, 0, s>>>(a);
+    else if (a.N == 5) k_grad<5><<<grid, 256, 0, s>>>(a);
+    else k_grad<6><<<grid, 256, 0, s>>>(a);
+}
+
+// FP64 stack of the shots' gradients over the interior, shots in order.
+__global__ void k_grad_stack(const GradStackArgs a) {
+    const int nz = a.Z - 2 * a.L;
+    const int ii = blockIdx.y, i = ii + a.L;
+    for (int jj = threadIdx.x + blockIdx.x * blockDim.x; jj < nz; jj += blockDim.x * gridDim.x) {
+        const ptrdiff_t g = (ptrdiff_t)i * a.pitch + jj + a.L;
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < a.nshots; ++b)
+            for (int k = 0; k < 3; ++k) s[k] += (double)a.g[k][(size_t)b * a.grad_stride + g];
+        for (int k = 0; k < 3; ++k) a.stack[k][(size_t)ii * nz + jj] += s[k];
+    }
+}
+
+void launch_grad_stack(const GradStackArgs& a, cudaStream_t s) {
+    const int nz = a.Z - 2 * a.L, nx = a.X - 2 * a.L;
+    k_grad_stack<<<dim3((nz + 255) / 256, nx), 256, 0, s>>>(a);
+}
+
 struct PackArgs {
     const float* f[12];
     int nf, X, Z, pitch;

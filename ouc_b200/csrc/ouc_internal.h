@@ -176,6 +176,28 @@ struct SnapArgs {
     int comp_image;
 };
 
+// FWI gradient of one back-step (see k_grad).
+struct GradArgs {
+    int X, Z, pitch, L, N;
+    int nshots;
+    float a[6];
+    float dx, dz;
+    const float* src[4];     // source Px Pz Sx Sz at the imaged level (shot 0)
+    const float* rcv[4];     // receiver Px Pz Sx Sz after the back-step (shot 0)
+    size_t shot_stride;      // state floats between shots
+    const float* vp;         // Vp, Vs and (or null: 1) rho of the formula
+    const float* vs;
+    const float* rho;
+    float* g[3];             // shot 0: gradient w.r.t. Vp, w.r.t. Vs, source illumination
+    size_t grad_stride;      // floats between shots' gradient accumulators
+};
+struct GradStackArgs {
+    int X, Z, pitch, L, nshots;
+    const float* g[3];
+    size_t grad_stride;
+    double* stack[3];        // nx*nz dense FP64
+};
+
 // Host-side launchers (kernels.cu)
 int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s);
 void configure_step_kernels(int N);
@@ -189,5 +211,7 @@ void launch_pack_fields(const float* const* f, int nf, int X, int Z, int pitch, 
 void launch_strip_pack(const ShotDesc* shots, int nshots, int slot, int ring, size_t strip_slot, cudaStream_t s);
 void launch_snap_store(const SnapArgs& a, int nshots, cudaStream_t s);
 void launch_image_snap(const SnapArgs& a, int nshots, cudaStream_t s);
+void launch_grad(const GradArgs& a, cudaStream_t s);
+void launch_grad_stack(const GradStackArgs& a, cudaStream_t s);
 
 }  // namespace ouc

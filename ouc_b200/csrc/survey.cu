@@ -59,6 +59,7 @@ struct Window {
 int check(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture* ap) {
     if (n < 1 || !shots || !ap) return fail(ctx, OUC_EINVAL, "no shots or apertures");
     if (ctx->cfg.snapshot_every > 0) return fail(ctx, OUC_EINVAL, "the survey runs the strip form (snapshot_every = 0)");
+    if (ctx->cfg.gradient) return fail(ctx, OUC_EINVAL, "the survey does not compute the FWI gradient");
     for (int k = 0; k < n; ++k) {
         int rc = check_shot(ctx, &shots[k]);
         if (rc) return rc;
