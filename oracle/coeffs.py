@@ -18,6 +18,9 @@ import sys
 import numpy as np
 
 REFERENCE_N6 = (1.2213364, -9.6931458e-2, 1.7447662e-2, -2.9672895e-3, 3.5900540e-4, -2.1847812e-5)
+# The reference's first-order velocity/stress kernels (P-S-seperating.cu:405,
+# 501) carry five-digit literals of the same weights.
+REFERENCE_FO_N6 = (1.2213e+0, -9.6931e-2, 1.7448e-2, -2.9673e-3, 3.5901e-4, -2.1848e-5)
 
 
 def exact(n):
@@ -37,6 +40,12 @@ def float32_weights(n):
     if n == 6:
         return [np.float32(v) for v in REFERENCE_N6]
     return [np.float32(float(v)) for v in exact(n)]
+
+
+def float32_weights_first_order(n):
+    if n == 6:
+        return [np.float32(v) for v in REFERENCE_FO_N6]
+    return float32_weights(n)
 
 
 if __name__ == "__main__":

@@ -572,6 +572,112 @@ struct Engine {
     }
 };
 
+// ---- first-order velocity-stress scheme ------------------------------------
+// The reference's stress (PS:487-560) and velocity (PS:390-486) kernels, which
+// its main() never calls.  One step: stress (velocity derivatives -> split
+// stresses with the split-field damping (1 - dt a/2) / (1 + dt a/2), source on
+// theta), then velocity (stress derivatives -> P/S velocities, U = P + S,
+// receiver row recorded after the update).  The damping factors and the
+// update are evaluated in double precision and rounded once, as the
+// reference's double literals make them; powf(v, 2) as written there.
+template <class T>
+struct FoWave {
+    int X = 0, Z = 0;
+    Field<T> vx, vz, vpx, vpz, vsx, vsz, th, om, qzx, qzz, qxx, qxz, thx, thz, omx, omz;
+    void init(int x, int z) {
+        X = x; Z = z;
+        for (Field<T>* f : {&vx, &vz, &vpx, &vpz, &vsx, &vsz, &th, &om, &qzx, &qzz, &qxx, &qxz, &thx, &thz, &omx, &omz})
+            f->init(x, z);
+    }
+};
+
+inline float fo_sq(float v) { return powf(v, 2); }
+inline double fo_sq(double v) { return v * v; }
+
+template <class T>
+inline T fo_damped(T a, T dt, double term, T old) {
+    const double h = 0.5 * (double)dt * (double)a;
+    return (T)((1.0 / (1.0 + h)) * (term + (1.0 - h) * (double)old));
+}
+
+template <class T>
+inline void fo_stress_cell(FoWave<T>& w, const Model<T>& m, const T* a, int N, T dx, T dz, T dt, int i, int j,
+                           T srcval) {
+    const int Z = w.Z;
+    const size_t c = (size_t)i * Z + j;
+    const T exx = dminus(w.vx.p() + c, (ptrdiff_t)Z, a, N, dx);   // dvxdx
+    const T exz = dplus(w.vx.p() + c, (ptrdiff_t)1, a, N, dz);    // dvxdz
+    const T ezz = dminus(w.vz.p() + c, (ptrdiff_t)1, a, N, dz);   // dvzdz
+    const T ezx = dplus(w.vz.p() + c, (ptrdiff_t)Z, a, N, dx);    // dvzdx
+    const T vp2 = fo_sq(m.vp.v[c]), vs2 = fo_sq(m.vs.v[c]);
+    const T ax = m.ax.v[c], az = m.az.v[c];
+    w.thx.v[c] = fo_damped(ax, dt, (double)(dt * vp2 * exx), w.thx.v[c]);
+    w.thz.v[c] = fo_damped(az, dt, (double)(dt * vp2 * ezz), w.thz.v[c]);
+    w.omx.v[c] = fo_damped(ax, dt, (double)(-dt * vs2 * ezx), w.omx.v[c]);
+    w.omz.v[c] = fo_damped(az, dt, (double)(dt * vs2 * exz), w.omz.v[c]);
+    w.qxx.v[c] = fo_damped(ax, dt, (double)(dt * vs2 * exx), w.qxx.v[c]);
+    w.qxz.v[c] = fo_damped(az, dt, (double)(dt * vs2 * exz), w.qxz.v[c]);
+    w.qzx.v[c] = fo_damped(ax, dt, (double)(dt * vs2 * ezx), w.qzx.v[c]);
+    w.qzz.v[c] = fo_damped(az, dt, (double)(dt * vs2 * ezz), w.qzz.v[c]);
+    w.th.v[c] = w.thx.v[c] + w.thz.v[c] + srcval;
+    w.om.v[c] = w.omx.v[c] + w.omz.v[c];
+}
+
+template <class T>
+inline void fo_velocity_cell(FoWave<T>& w, const Model<T>& m, const T* a, int N, T dx, T dz, T dt, int i, int j) {
+    const ptrdiff_t Z = w.Z;
+    const size_t c = (size_t)i * Z + j;
+    const T tx = dplus(w.th.p() + c, Z, a, N, dx), tz = dplus(w.th.p() + c, (ptrdiff_t)1, a, N, dz);
+    const T wx = dminus(w.om.p() + c, Z, a, N, dx), wz = dminus(w.om.p() + c, (ptrdiff_t)1, a, N, dz);
+    const T dux_xdz = dplus(w.qxx.p() + c, (ptrdiff_t)1, a, N, dz);
+    const T dux_zdx = dminus(w.qxz.p() + c, Z, a, N, dx);
+    const T duz_xdz = dminus(w.qzx.p() + c, (ptrdiff_t)1, a, N, dz);
+    const T duz_zdx = dplus(w.qzz.p() + c, Z, a, N, dx);
+    const T ax = m.ax.v[c], az = m.az.v[c];
+    auto upd = [&](T damp, T old, T sum) {
+        const double h = 0.5 * (double)dt * (double)damp;
+        return (T)((1.0 / (1.0 + h)) * ((1 - h) * (double)old + (double)(dt * sum)));
+    };
+    w.vpx.v[c] = upd(ax, w.vpx.v[c], tx + duz_xdz - duz_zdx);
+    w.vpz.v[c] = upd(az, w.vpz.v[c], tz + dux_zdx - dux_xdz);
+    w.vsx.v[c] = upd(ax, w.vsx.v[c], wz + duz_xdz - duz_zdx);
+    w.vsz.v[c] = upd(az, w.vsz.v[c], -wx + dux_zdx - dux_xdz);
+    w.vx.v[c] = w.vpx.v[c] + w.vsx.v[c];
+    w.vz.v[c] = w.vpz.v[c] + w.vsz.v[c];
+}
+
+template <class T>
+int run_forward_fo(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                   const float* src, T* rec_vx, T* rec_vz, T* fields_out) {
+    Engine<T> e;
+    e.setup(c, vp, vs, ax, az);
+    const int X = c->X, Z = c->Z, N = c->N, nt = c->nt;
+    FoWave<T> w;
+    w.init(X, Z);
+    for (int t = 0; t < nt; ++t) {
+#pragma omp parallel for schedule(static)
+        for (int i = N; i < X - N; ++i)
+            for (int j = N; j < Z - N; ++j) {
+                const T s = (i == c->sx && j == c->sz) ? (T)src[t] : T(0);
+                fo_stress_cell<T>(w, e.m, e.a, N, e.dx, e.dz, e.dt, i, j, s);
+            }
+#pragma omp parallel for schedule(static)
+        for (int i = N; i < X - N; ++i)
+            for (int j = N; j < Z - N; ++j) fo_velocity_cell<T>(w, e.m, e.a, N, e.dx, e.dz, e.dt, i, j);
+        for (int i = 0; i < X; ++i) {
+            if (rec_vx) rec_vx[(size_t)i * nt + t] = w.vx(i, c->rz);
+            if (rec_vz) rec_vz[(size_t)i * nt + t] = w.vz(i, c->rz);
+        }
+    }
+    if (fields_out) {
+        Field<T>* fs[16] = {&w.vx, &w.vz, &w.vpx, &w.vpz, &w.vsx, &w.vsz, &w.th, &w.om,
+                            &w.qzx, &w.qzz, &w.qxx, &w.qxz, &w.thx, &w.thz, &w.omx, &w.omz};
+        const size_t C = (size_t)X * Z;
+        for (int k = 0; k < 16; ++k) std::copy(fs[k]->v.begin(), fs[k]->v.end(), fields_out + k * C);
+    }
+    return 0;
+}
+
 template <class T>
 int run_forward(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
                 const float* src, T* rec_vx, T* rec_vz, T* fields_out, const float* rho = nullptr) {
@@ -640,6 +746,18 @@ int orc_rtm_grad_f32(const orc_cfg* c, const float* vp, const float* vs, const f
     e.grad_out = grad;
     e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, nullptr, nullptr, nullptr, nullptr, nullptr);
     return 0;
+}
+
+// First-order velocity-stress forward modeling (see run_forward_fo):
+// records X x nt, fields 16 x X x Z (Vx Vz Vpx Vpz Vsx Vsz theta omega Qzx
+// Qzz Qxx Qxz theta_x theta_z omega_x omega_z).
+int orc_forward_fo_f32(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                       const float* src, float* rec_vx, float* rec_vz, float* fields_out) {
+    return run_forward_fo<float>(c, vp, vs, ax, az, src, rec_vx, rec_vz, fields_out);
+}
+int orc_forward_fo_f64(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                       const float* src, double* rec_vx, double* rec_vz, double* fields_out) {
+    return run_forward_fo<double>(c, vp, vs, ax, az, src, rec_vx, rec_vz, fields_out);
 }
 
 // Variable-density variants (rho: padded X x Z density; see Model).

@@ -52,6 +52,15 @@ def weights(n):
     return np.array(mod.float32_weights(n), dtype=np.float32)
 
 
+def weights_first_order(n):
+    """float32 weights of the reference's first-order kernels (oracle/coeffs.py)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("orc_coeffs", os.path.join(HERE, "coeffs.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return np.array(mod.float32_weights_first_order(n), dtype=np.float32)
+
+
 @dataclass
 class Shot:
     X: int
@@ -102,6 +111,10 @@ class Oracle:
         self.lib.orc_rtm_rho_f64.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _dp, _dp, _dp,
                                              _dp, _dp, _dp, _dp]
         self.lib.orc_rtm_rho_f64.restype = C.c_int
+        for name, t in (("orc_forward_fo_f32", _fp), ("orc_forward_fo_f64", _dp)):
+            f = getattr(self.lib, name)
+            f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, t, t, t]
+            f.restype = C.c_int
         for name, t in (("orc_rtm_grad_f32", _fp), ("orc_rtm_grad_f64", _dp)):
             f = getattr(self.lib, name)
             f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, t, t, t]
@@ -142,6 +155,23 @@ class Oracle:
             assert rc == 0
             return rx, rz, fields
         f = self.lib.orc_forward_f64 if fp64 else self.lib.orc_forward_f32
+        rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx, dt), _ptr(rz, dt),
+               _ptr(fields, dt))
+        assert rc == 0
+        return rx, rz, fields
+
+    def forward_fo(self, shot: Shot, vp, vs, ax, az, src, fp64=False):
+        """First-order velocity-stress forward modeling (the reference's
+        stress/velocity kernels): (rec_vx, rec_vz, fields[16])."""
+        dt = np.float64 if fp64 else np.float32
+        X, Z, nt = shot.X, shot.Z, shot.nt
+        rx = np.zeros((X, nt), dt)
+        rz = np.zeros((X, nt), dt)
+        fields = np.zeros((16, X, Z), dt)
+        c = shot.cfg()
+        for k, w in enumerate(weights_first_order(shot.N)):
+            c.coeff[k] = float(w)
+        f = self.lib.orc_forward_fo_f64 if fp64 else self.lib.orc_forward_fo_f32
         rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx, dt), _ptr(rz, dt),
                _ptr(fields, dt))
         assert rc == 0
@@ -211,6 +241,8 @@ class RefBuild:
         self.lib.psr_forward.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, _fp, _fp, _fp,
                                          _fp, _fp, C.c_int, _fp, _fp, _fp, _fp]
         self.lib.psr_forward.restype = C.c_int
+        self.lib.psr_forward_fo.argtypes = self.lib.psr_forward.argtypes
+        self.lib.psr_forward_fo.restype = C.c_int
         self.lib.psr_rtm_shot.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                           C.c_float, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _fp, _fp, _fp,
                                           _fp, _fp, _fp, _fp, _fp]
@@ -231,6 +263,20 @@ class RefBuild:
         ms = np.zeros(1, np.float32)
         rc = self.lib.psr_forward(sx, sz, rz, dt, dx, dz, _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src_full),
                                   nt_run, _ptr(rx), _ptr(rzr), _ptr(fields), _ptr(ms))
+        assert rc == 0, rc
+        return rx[:, :nt_run], rzr[:, :nt_run], fields, float(ms[0])
+
+    def forward_fo(self, sx, sz, rz, dt, dx, dz, vp, vs, ax, az, src, nt_run):
+        """The reference's first-order stress + velocity kernels: (rec_vx, rec_vz, fields[16], ms)."""
+        X, Z, NT = self.X, self.Z, self.NT
+        src_full = np.zeros(NT, np.float32)
+        src_full[: len(src)] = src[:NT]
+        rx = np.zeros((X, NT), np.float32)
+        rzr = np.zeros((X, NT), np.float32)
+        fields = np.zeros((16, X, Z), np.float32)
+        ms = np.zeros(1, np.float32)
+        rc = self.lib.psr_forward_fo(sx, sz, rz, dt, dx, dz, _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src_full),
+                                     nt_run, _ptr(rx), _ptr(rzr), _ptr(fields), _ptr(ms))
         assert rc == 0, rc
         return rx[:, :nt_run], rzr[:, :nt_run], fields, float(ms[0])
 

@@ -77,6 +77,36 @@ def test_oracle_bit_exact_vs_reference_kernels_other_geometry(oracle):
         assert np.array_equal(r[k], o[k]), k
 
 
+@pytest.mark.parametrize("name", ["g64n6", "g72x56n5", "g48x40n2"])
+def test_first_order_oracle_bit_exact_vs_reference_kernels(oracle, name):
+    """The first-order velocity-stress scheme (the reference's stress and
+    velocity kernels, never called by its main()): the oracle's float build
+    against those kernels run on the CPU, gathers and all 16 fields."""
+    if not os.path.exists(os.path.join(REF_DIR, f"libpsref_emu_{name}.so")):
+        pytest.skip("reference CPU build not present (needs the reference sources)")
+    ref = RefBuild(name, "emu")
+    X, Z, L, N, NT = ref.X, ref.Z, ref.L, ref.N, ref.NT
+    rng = np.random.default_rng(11)
+    vp = np.zeros((X, Z), np.float32)
+    vs = np.zeros((X, Z), np.float32)
+    vp[L:X - L, L:Z - L] = rng.uniform(2000, 3500, (X - 2 * L, Z - 2 * L))
+    vs[L:X - L, L:Z - L] = vp[L:X - L, L:Z - L] / 1.8
+    _, vp, vs = ref.pad(np.ones_like(vp), vp, vs)
+    ax, az = oracle.profile(vp, L)
+    src = np.sin(np.arange(NT) * 0.2).astype(np.float32) * np.exp(-np.arange(NT) / 40.0).astype(np.float32)
+    from oracle.oracle import Shot
+    sh = Shot(X=X, Z=Z, L=L, N=N, nt=NT, sx=L + 17, sz=L + 5, rz=L + 2, dx=8.0, dz=8.0, dt=6e-4)
+    rx, rz, rf, _ = ref.forward_fo(sh.sx, sh.sz, sh.rz, np.float32(6e-4), np.float32(8.0), np.float32(8.0), vp, vs,
+                                   ax, az, src, NT)
+    ox, oz, of = oracle.forward_fo(sh, vp, vs, ax, az, src)
+    assert np.abs(rx).max() > 0
+    assert np.array_equal(rx, ox) and np.array_equal(rz, oz)
+    for k in range(16):
+        assert np.array_equal(rf[k], of[k]), k
+    dx_, dz_, df = oracle.forward_fo(sh, vp, vs, ax, az, src, fp64=True)
+    assert rel_l2(rx, dx_) < 1e-5
+
+
 def test_padding_matches_reference(oracle):
     """orc_pad_model restates xiangbian (PS:37-119); compare with the fixture's padded model."""
     g = load_golden("g72x56n5")
