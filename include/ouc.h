@@ -153,6 +153,21 @@ int ouc_forward(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float*
 int ouc_forward_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, float* d_gather_vx,
                     float* d_gather_vz);
 
+/* Forward modeling with the first-order velocity-stress scheme of the
+ * reference's stress (PS:487-560) and velocity (PS:390-486) kernels, which
+ * its main() never calls: split stresses theta_x/z, omega_x/z and the four Q
+ * fields with the split-field damping (1 - dt a/2)/(1 + dt a/2) of the
+ * context's profile, the wavelet added to theta at the source cell, P/S
+ * velocities updated from the stress derivatives, U = P + S recorded at the
+ * receiver row after the update (the receiver test as a comparison,
+ * PS:481).  Half-order 6 uses the kernels' own five-digit weights, other
+ * orders the context's.  Theta source only; density-normalised contexts
+ * only.  gather_vx/vz: X*nt each in cfg->gather_layout, or NULL.  fields:
+ * optional 16*X*Z output of the final Vx Vz Vpx Vpz Vsx Vsz theta omega
+ * duzdx duzdz duxdx duxdz theta_x theta_z omega_x omega_z. */
+int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gather_vx, float* gather_vz,
+                   float* fields);
+
 /* One RTM shot: forward with boundary-strip save (PS:2258-2292), optional
  * mute (PS:2293), receiver back-propagation with record injection and the
  * source-wavefield reconstruction (PS:2313-2364), PP/PS imaging (PS:2361),

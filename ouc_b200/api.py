@@ -173,6 +173,22 @@ class Context:
         check(lib().ouc_forward(self._h, C.byref(sc), _p(w), _p(gx), _p(gz), _p(f)), self._h)
         return gx, gz, f
 
+    def forward_first_order(self, shot: Shot, wavelet, fields=False):
+        """Forward modeling with the first-order velocity-stress scheme (the
+        reference's stress/velocity kernels, P-S-seperating.cu:390-560):
+        (gather_vx, gather_vz, fields or None).
+
+        fields: final Vx Vz Vpx Vpz Vsx Vsz theta omega duzdx duzdz duxdx duxdz
+        theta_x theta_z omega_x omega_z on the padded grid, (16, X, Z)."""
+        w = _f32(wavelet)
+        assert w.shape == (self.cfg.nt,)
+        gx = np.zeros(self._gshape(), np.float32)
+        gz = np.zeros(self._gshape(), np.float32)
+        f = np.zeros((16, self.X, self.Z), np.float32) if fields else None
+        sc = shot.c()
+        check(lib().ouc_forward_fo(self._h, C.byref(sc), _p(w), _p(gx), _p(gz), _p(f)), self._h)
+        return gx, gz, f
+
     def rtm_shot(self, shot: Shot, wavelet, rec=None):
         """One RTM shot; rec = (rec_vx, rec_vz) in the configured gather layout,
         or None to migrate the records this shot's own forward pass produces."""
