@@ -167,6 +167,15 @@ int ouc_forward_dev(ouc_ctx* ctx, const ouc_shot* shot, const float* d_wavelet, 
  * duzdx duzdz duxdx duxdz theta_x theta_z omega_x omega_z. */
 int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gather_vx, float* gather_vz,
                    float* fields);
+/* Receiver back-propagation with the same first-order scheme: the
+ * reference's stress_backward_propagation (PS:821-887) and
+ * velocity_backward_propagation (PS:728-820), i.e. the updates above without
+ * source and record, for t = nt-1 .. 0, each step preceded by the records of
+ * time t written into U at the receiver row on the interior columns [L, X-L)
+ * (load_record, PS:1472-1481, as the launched receiver path orders it,
+ * PS:2319).  rec_vx/rec_vz: X*nt each in cfg->gather_layout.  fields: as
+ * ouc_forward_fo (theta without a source term). */
+int ouc_backward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* rec_vx, const float* rec_vz, float* fields);
 
 /* One RTM shot: forward with boundary-strip save (PS:2258-2292), optional
  * mute (PS:2293), receiver back-propagation with record injection and the

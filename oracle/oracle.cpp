@@ -12,7 +12,7 @@
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
 // this library, and only as a checker or a timed CPU baseline.
 //
-// Parity is pinned: tests/test_oracle_pin.py compares this file's float
+// Parity is pinned: tests/test_oracle.py compares this file's float
 // instantiation bit-for-bit with the reference's own kernels compiled for the
 // CPU from the reference sources (oracle/refemu, oracle/Makefile).
 //
@@ -678,6 +678,41 @@ int run_forward_fo(const orc_cfg* c, const float* vp, const float* vs, const flo
     return 0;
 }
 
+// First-order receiver back-propagation: the reference's
+// stress_backward_propagation (PS:821-887) and velocity_backward_propagation
+// (PS:728-820) are the stress/velocity updates without source and record;
+// before each step (t = nt-1 .. 0) the receiver row of U is replaced by the
+// records on [L, X-L), as load_record (PS:1472-1481) does in the launched
+// receiver path (PS:2319).  rec_*: X x nt.
+template <class T>
+int run_backward_fo(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                    const float* rec_vx, const float* rec_vz, T* fields_out) {
+    Engine<T> e;
+    e.setup(c, vp, vs, ax, az);
+    const int X = c->X, Z = c->Z, N = c->N, L = c->L, nt = c->nt;
+    FoWave<T> w;
+    w.init(X, Z);
+    for (int t = nt - 1; t >= 0; --t) {
+        for (int i = L; i < X - L; ++i) {
+            w.vx(i, c->rz) = (T)rec_vx[(size_t)i * nt + t];
+            w.vz(i, c->rz) = (T)rec_vz[(size_t)i * nt + t];
+        }
+#pragma omp parallel for schedule(static)
+        for (int i = N; i < X - N; ++i)
+            for (int j = N; j < Z - N; ++j) fo_stress_cell<T>(w, e.m, e.a, N, e.dx, e.dz, e.dt, i, j, T(0));
+#pragma omp parallel for schedule(static)
+        for (int i = N; i < X - N; ++i)
+            for (int j = N; j < Z - N; ++j) fo_velocity_cell<T>(w, e.m, e.a, N, e.dx, e.dz, e.dt, i, j);
+    }
+    if (fields_out) {
+        Field<T>* fs[16] = {&w.vx, &w.vz, &w.vpx, &w.vpz, &w.vsx, &w.vsz, &w.th, &w.om,
+                            &w.qzx, &w.qzz, &w.qxx, &w.qxz, &w.thx, &w.thz, &w.omx, &w.omz};
+        const size_t C = (size_t)X * Z;
+        for (int k = 0; k < 16; ++k) std::copy(fs[k]->v.begin(), fs[k]->v.end(), fields_out + k * C);
+    }
+    return 0;
+}
+
 template <class T>
 int run_forward(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
                 const float* src, T* rec_vx, T* rec_vz, T* fields_out, const float* rho = nullptr) {
@@ -758,6 +793,15 @@ int orc_forward_fo_f32(const orc_cfg* c, const float* vp, const float* vs, const
 int orc_forward_fo_f64(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
                        const float* src, double* rec_vx, double* rec_vz, double* fields_out) {
     return run_forward_fo<double>(c, vp, vs, ax, az, src, rec_vx, rec_vz, fields_out);
+}
+// First-order receiver back-propagation (see run_backward_fo).
+int orc_backward_fo_f32(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                        const float* rec_vx, const float* rec_vz, float* fields_out) {
+    return run_backward_fo<float>(c, vp, vs, ax, az, rec_vx, rec_vz, fields_out);
+}
+int orc_backward_fo_f64(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                        const float* rec_vx, const float* rec_vz, double* fields_out) {
+    return run_backward_fo<double>(c, vp, vs, ax, az, rec_vx, rec_vz, fields_out);
 }
 
 // Variable-density variants (rho: padded X x Z density; see Model).

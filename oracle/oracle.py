@@ -115,6 +115,10 @@ class Oracle:
             f = getattr(self.lib, name)
             f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, t, t, t]
             f.restype = C.c_int
+        for name, t in (("orc_backward_fo_f32", _fp), ("orc_backward_fo_f64", _dp)):
+            f = getattr(self.lib, name)
+            f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, t]
+            f.restype = C.c_int
         for name, t in (("orc_rtm_grad_f32", _fp), ("orc_rtm_grad_f64", _dp)):
             f = getattr(self.lib, name)
             f.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, t, t, t]
@@ -176,6 +180,21 @@ class Oracle:
                _ptr(fields, dt))
         assert rc == 0
         return rx, rz, fields
+
+    def backward_fo(self, shot: Shot, vp, vs, ax, az, rec_vx, rec_vz, fp64=False):
+        """First-order receiver back-propagation (the reference's
+        *_backward_propagation kernels, records injected at the receiver row
+        for t = nt-1 .. 0): fields[16] after the step at t = 0.  rec_*: X x nt."""
+        dt = np.float64 if fp64 else np.float32
+        fields = np.zeros((16, shot.X, shot.Z), dt)
+        c = shot.cfg()
+        for k, w in enumerate(weights_first_order(shot.N)):
+            c.coeff[k] = float(w)
+        f = self.lib.orc_backward_fo_f64 if fp64 else self.lib.orc_backward_fo_f32
+        rc = f(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(np.ascontiguousarray(rec_vx, np.float32)),
+               _ptr(np.ascontiguousarray(rec_vz, np.float32)), _ptr(fields, dt))
+        assert rc == 0
+        return fields
 
     def rtm(self, shot: Shot, vp, vs, ax, az, src, rec=None, fp64=False, rho=None):
         """rho (padded density): the variable-density extension, FP64 only."""
@@ -243,6 +262,9 @@ class RefBuild:
         self.lib.psr_forward.restype = C.c_int
         self.lib.psr_forward_fo.argtypes = self.lib.psr_forward.argtypes
         self.lib.psr_forward_fo.restype = C.c_int
+        self.lib.psr_backward_fo.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, _fp, _fp, _fp, _fp, _fp, _fp,
+                                             C.c_int, _fp, _fp]
+        self.lib.psr_backward_fo.restype = C.c_int
         self.lib.psr_rtm_shot.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                           C.c_float, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _fp, _fp, _fp,
                                           _fp, _fp, _fp, _fp, _fp]
@@ -279,6 +301,21 @@ class RefBuild:
                                      nt_run, _ptr(rx), _ptr(rzr), _ptr(fields), _ptr(ms))
         assert rc == 0, rc
         return rx[:, :nt_run], rzr[:, :nt_run], fields, float(ms[0])
+
+    def backward_fo(self, rz, dt, dx, dz, vp, vs, ax, az, rec_vx, rec_vz, nt_run):
+        """The reference's first-order backward-propagation kernels with
+        load_record injection: (fields[16], ms).  rec_*: X x nt_run."""
+        X, Z, NT = self.X, self.Z, self.NT
+        rx = np.zeros((X, NT), np.float32)
+        rzz = np.zeros((X, NT), np.float32)
+        rx[:, :nt_run] = rec_vx
+        rzz[:, :nt_run] = rec_vz
+        fields = np.zeros((16, X, Z), np.float32)
+        ms = np.zeros(1, np.float32)
+        rc = self.lib.psr_backward_fo(rz, dt, dx, dz, _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(rx), _ptr(rzz),
+                                      nt_run, _ptr(fields), _ptr(ms))
+        assert rc == 0, rc
+        return fields, float(ms[0])
 
     def rtm(self, sx, sz, rz, t0, dt, dx, dz, vp, vs, ax, az, src, rec=None, do_mute=1):
         X, Z, NT, L = self.X, self.Z, self.NT, self.L

@@ -58,6 +58,7 @@ SIGNATURES = {
     "ouc_forward": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp, _fp]),
     "ouc_forward_dev": (C.c_int, [_vp, C.POINTER(ouc_shot), _vp, _vp, _vp]),
     "ouc_forward_fo": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp, _fp]),
+    "ouc_backward_fo": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp]),
     "ouc_rtm_shot": (C.c_int, [_vp, C.POINTER(ouc_shot), _fp, _fp, _fp, _fp, _fp]),
     "ouc_rtm_shot_dev": (C.c_int, [_vp, C.POINTER(ouc_shot), _vp, _vp, _vp, _vp, _vp]),
     "ouc_rtm_batch": (C.c_int, [_vp, C.c_int, C.POINTER(ouc_shot), _fp, C.POINTER(_fp), C.POINTER(_fp),

@@ -189,6 +189,19 @@ class Context:
         check(lib().ouc_forward_fo(self._h, C.byref(sc), _p(w), _p(gx), _p(gz), _p(f)), self._h)
         return gx, gz, f
 
+    def backward_first_order(self, shot: Shot, rec_vx, rec_vz):
+        """Receiver back-propagation with the first-order scheme (the
+        reference's *_backward_propagation kernels, P-S-seperating.cu:728-887,
+        records written into U at the receiver row before each step, t = nt-1
+        .. 0); rec_* in the configured gather layout.  Returns the final
+        fields, (16, X, Z), in the order of forward_first_order."""
+        rx, rz = _f32(rec_vx), _f32(rec_vz)
+        assert rx.shape == self._gshape() and rz.shape == self._gshape()
+        f = np.zeros((16, self.X, self.Z), np.float32)
+        sc = shot.c()
+        check(lib().ouc_backward_fo(self._h, C.byref(sc), _p(rx), _p(rz), _p(f)), self._h)
+        return f
+
     def rtm_shot(self, shot: Shot, wavelet, rec=None):
         """One RTM shot; rec = (rec_vx, rec_vz) in the configured gather layout,
         or None to migrate the records this shot's own forward pass produces."""

@@ -787,7 +787,7 @@ int ouc_destroy(ouc_ctx* ctx) {
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
     cudaFree(ctx->l_in); cudaFree(ctx->l_out); cudaFree(ctx->l_truth); cudaFree(ctx->l_scale); cudaFree(ctx->l_tmp); cudaFree(ctx->sv_model);
-    cudaFree(ctx->grad);
+    cudaFree(ctx->grad); cudaFree(ctx->fo_sq);
     for (auto* p : ctx->d_gstack) cudaFree(p);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);

@@ -98,6 +98,8 @@ struct ouc_ctx {
     float* l_tmp = nullptr;      // [X][Z][OUC_CNN_OUT] smoothing scratch
     // survey (survey.cu): per-slot sub-grid models [batch][4 fields] (vp2 vs2 ax az)
     float* sv_model = nullptr;
+    // first-order scheme (fo.cu): powf(Vp, 2), powf(Vs, 2) in the model layout, allocated on first use
+    float* fo_sq = nullptr;
     size_t bytes = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 

@@ -38,13 +38,16 @@ struct FoArgs {
     float* vnew[4];
     const float* sold[8];            // theta_x theta_z omega_x omega_z Qxx Qxz Qzx Qzz
     float* snew[8];
-    const float* vp;                 // Vp, Vs (not squared), damping x, z
-    const float* vs;
+    const float* vp2;                // powf(Vp, 2), powf(Vs, 2) (k_squares), damping x, z
+    const float* vs2;
     const float* ax;
     const float* az;
-    const float* wavelet;
+    const float* wavelet;            // source samples, or null (back-propagation)
     float* rec_x;                    // gather row t (time-major), or null
     float* rec_z;
+    const float* inj_x;              // records injected into U at the receiver
+    const float* inj_z;              // row on [L, X-L) (row t), or null
+    int L;
 };
 
 // split-field stress update, the reference's expression (PS:547-556)
@@ -54,6 +57,24 @@ __device__ __forceinline__ float stress_upd(float damp, float dt, float term, fl
 // velocity update, the reference's expression (PS:471-474)
 __device__ __forceinline__ float vel_upd(float damp, float dt, float old, float sum) {
     return (1.0 / (1.0 + 0.5 * dt * damp)) * ((1 - 0.5 * dt * damp) * old + dt * sum);
+}
+// Both updates where the damping is 0 (the interior): the factors are exactly
+// 1, and the double sum of two floats rounded to float is their float sum
+// (53 >= 2*24 + 2: the double rounding is innocuous), so the result is one
+// float addition -- bit-identical, without the double arithmetic.
+__device__ __forceinline__ bool undamped4(const float4& ax, const float4& az) {
+    return ax.x == 0.f && ax.y == 0.f && ax.z == 0.f && ax.w == 0.f && az.x == 0.f && az.y == 0.f && az.z == 0.f &&
+           az.w == 0.f;
+}
+
+// powf(v, 2) of the model once per call, as the kernels evaluate it per cell
+// (PS:547); guard cells hold 0.
+__global__ void k_squares(const float* __restrict__ vp, const float* __restrict__ vs, float* vp2, float* vs2,
+                          size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        vp2[k] = powf(vp[k], 2);
+        vs2[k] = powf(vs[k], 2);
+    }
 }
 
 template <int N>
@@ -85,8 +106,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
     for (int idx = tid; idx < G::UR * (UC / 4); idx += kThreads) {
         const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
         const ptrdiff_t g = (ptrdiff_t)(ux_i0 + r) * P + (ux_j0 + 4 * c4);
-        st4(sUx + r * UC + 4 * c4, add4(ld4(p.vold[0] + g), ld4(p.vold[2] + g)));   // Vx = Vpx + Vsx
-        st4(sUz + r * UC + 4 * c4, add4(ld4(p.vold[1] + g), ld4(p.vold[3] + g)));
+        float4 ux = add4(ld4(p.vold[0] + g), ld4(p.vold[2] + g));   // Vx = Vpx + Vsx
+        float4 uz = add4(ld4(p.vold[1] + g), ld4(p.vold[3] + g));
+        const int gi = ux_i0 + r, gj = ux_j0 + 4 * c4;
+        if (p.inj_x && p.rz >= gj && p.rz < gj + 4 && gi >= p.L && gi < p.X - p.L) {
+            // load_record (PS:1472-1481): U at the receiver row replaced by
+            // the records before the stress update reads it
+            set_comp(ux, p.rz - gj, p.inj_x[gi]);
+            set_comp(uz, p.rz - gj, p.inj_z[gi]);
+        }
+        st4(sUx + r * UC + 4 * c4, ux);
+        st4(sUz + r * UC + 4 * c4, uz);
     }
     __syncthreads();
 
@@ -115,34 +145,44 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
             const float4 exz = dz4<N, true>(ux0 + q * UC, a, dvz);    // dvxdz = D+z Vx
             const float4 ezz = dz4<N, false>(uz0 + q * UC, a, dvz);   // dvzdz = D-z Vz
             const ptrdiff_t g = (ptrdiff_t)gi * P + gjb;
-            const float4 vp = ld4(p.vp + g), vs = ld4(p.vs + g), axv = ld4(p.ax + g), azv = ld4(p.az + g);
+            const float4 vp2v = ld4(p.vp2 + g), vs2v = ld4(p.vs2 + g), axv = ld4(p.ax + g), azv = ld4(p.az + g);
             float4 so[8], sn[8];
 #pragma unroll
             for (int f = 0; f < 8; ++f) so[f] = ld4(p.sold[f] + g);
             const bool row_live = gi >= N && gi < p.X - N;
+            const bool flat = undamped4(axv, azv);
             float th[4], om[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int gj = gjb + k;
                 const bool live = row_live && gj >= N && gj < p.Z - N;
-                const float vp2 = powf(comp(vp, k), 2), vs2 = powf(comp(vs, k), 2);
-                const float dax = comp(axv, k), daz = comp(azv, k);
+                const float cp = __fmul_rn(dt, comp(vp2v, k)), cs = __fmul_rn(dt, comp(vs2v, k));
                 const float dxx = comp(exx[q], k), dzz = comp(ezz, k), dxz = comp(exz, k), dzx = comp(ezx[q], k);
+                // dt Vp^2 d, dt Vs^2 d and -dt Vs^2 d, each rounded as the reference's float products
+                float term[8];
+                term[0] = __fmul_rn(cp, dxx);    // theta_x
+                term[1] = __fmul_rn(cp, dzz);    // theta_z
+                term[2] = __fmul_rn(-cs, dzx);   // omega_x
+                term[3] = __fmul_rn(cs, dxz);    // omega_z
+                term[4] = __fmul_rn(cs, dxx);    // Qxx (duxdx)
+                term[5] = __fmul_rn(cs, dxz);    // Qxz (duxdz)
+                term[6] = __fmul_rn(cs, dzx);    // Qzx (duzdx)
+                term[7] = __fmul_rn(cs, dzz);    // Qzz (duzdz)
                 float v[8];
-                v[0] = stress_upd(dax, dt, dt * vp2 * dxx, comp(so[0], k));    // theta_x
-                v[1] = stress_upd(daz, dt, dt * vp2 * dzz, comp(so[1], k));    // theta_z
-                v[2] = stress_upd(dax, dt, -dt * vs2 * dzx, comp(so[2], k));   // omega_x
-                v[3] = stress_upd(daz, dt, dt * vs2 * dxz, comp(so[3], k));    // omega_z
-                v[4] = stress_upd(dax, dt, dt * vs2 * dxx, comp(so[4], k));    // Qxx (duxdx)
-                v[5] = stress_upd(daz, dt, dt * vs2 * dxz, comp(so[5], k));    // Qxz (duxdz)
-                v[6] = stress_upd(dax, dt, dt * vs2 * dzx, comp(so[6], k));    // Qzx (duzdx)
-                v[7] = stress_upd(daz, dt, dt * vs2 * dzz, comp(so[7], k));    // Qzz (duzdz)
+                if (flat) {
+#pragma unroll
+                    for (int f = 0; f < 8; ++f) v[f] = __fadd_rn(term[f], comp(so[f], k));
+                } else {
+                    const float dax = comp(axv, k), daz = comp(azv, k);
+#pragma unroll
+                    for (int f = 0; f < 8; ++f) v[f] = stress_upd((f & 1) ? daz : dax, dt, term[f], comp(so[f], k));
+                }
 #pragma unroll
                 for (int f = 0; f < 8; ++f) {
                     if (!live) v[f] = 0.f;   // the reference never updates these cells
                     set_comp(sn[f], k, v[f]);
                 }
-                const float s = (live && gi == p.sx && gj == p.sz) ? p.wavelet[p.t] : 0.f;
+                const float s = (p.wavelet && live && gi == p.sx && gj == p.sz) ? p.wavelet[p.t] : 0.f;
                 th[k] = v[0] + v[1] + s;   // PS:557
                 om[k] = v[2] + v[3];
             }
@@ -189,16 +229,29 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
             const float4 osx = ld4(p.vold[2] + g), osz = ld4(p.vold[3] + g);
             float4 npx, npz, nsx, nsz;
             const bool row_live = gi >= N && gi < p.X - N;
+            const bool flat = undamped4(axv, azv);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int gj = z0 + c + k;
                 const bool live = row_live && gj >= N && gj < p.Z - N;
-                const float dax = comp(axv, k), daz = comp(azv, k);
                 const float C = comp(dC, k), E = comp(dE[0], k), A = comp(dA, k), B = comp(dB[0], k);
-                float vpx = vel_upd(dax, dt, comp(opx, k), comp(txv[0], k) + C - E);
-                float vpz = vel_upd(daz, dt, comp(opz, k), comp(tzv, k) + B - A);
-                float vsx = vel_upd(dax, dt, comp(osx, k), comp(wzv, k) + C - E);
-                float vsz = vel_upd(daz, dt, comp(osz, k), -comp(wxv[0], k) + B - A);
+                const float sum_px = __fsub_rn(__fadd_rn(comp(txv[0], k), C), E);
+                const float sum_pz = __fsub_rn(__fadd_rn(comp(tzv, k), B), A);
+                const float sum_sx = __fsub_rn(__fadd_rn(comp(wzv, k), C), E);
+                const float sum_sz = __fsub_rn(__fadd_rn(-comp(wxv[0], k), B), A);
+                float vpx, vpz, vsx, vsz;
+                if (flat) {
+                    vpx = __fadd_rn(comp(opx, k), __fmul_rn(dt, sum_px));
+                    vpz = __fadd_rn(comp(opz, k), __fmul_rn(dt, sum_pz));
+                    vsx = __fadd_rn(comp(osx, k), __fmul_rn(dt, sum_sx));
+                    vsz = __fadd_rn(comp(osz, k), __fmul_rn(dt, sum_sz));
+                } else {
+                    const float dax = comp(axv, k), daz = comp(azv, k);
+                    vpx = vel_upd(dax, dt, comp(opx, k), sum_px);
+                    vpz = vel_upd(daz, dt, comp(opz, k), sum_pz);
+                    vsx = vel_upd(dax, dt, comp(osx, k), sum_sx);
+                    vsz = vel_upd(daz, dt, comp(osz, k), sum_sz);
+                }
                 if (!live) vpx = vpz = vsx = vsz = 0.f;
                 set_comp(npx, k, vpx); set_comp(npz, k, vpz); set_comp(nsx, k, vsx); set_comp(nsz, k, vsz);
             }
@@ -236,25 +289,40 @@ constexpr float kFoWeights6[6] = {(float)1.2213e+0, (float)-9.6931e-2, (float)1.
 using namespace ouc;
 using namespace ouc::host;
 
-extern "C" {
+namespace {
 
-int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gather_vx, float* gather_vz,
-                   float* fields) {
+int fo_check(ouc_ctx* ctx, const ouc_shot* shot) {
     if (!ctx) return OUC_EINVAL;
     int rc = check_shot(ctx, shot);
     if (rc) return rc;
-    if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
     if (shot->src_type != OUC_SRC_THETA) return fail(ctx, OUC_EINVAL, "the first-order scheme has the theta source only");
     if (ctx->cfg.density) return fail(ctx, OUC_EINVAL, "the first-order scheme is density-normalised");
-    cudaSetDevice(ctx->device);
-    ctx->step_phase = ouc_ctx::kIdle;
-    ctx->timing = ouc_timing{};
+    return OUC_OK;
+}
+
+// The first-order time loop on the source side's 24 fields (velocities
+// now[4] / past[4], stresses fo[4] + o[0..3] / fn[4] + o[4..7], ping-ponged
+// by step).  Forward: t = 0 .. nt-1 with the source and the record into the
+// context's gathers.  Backward: t = nt-1 .. 0 injecting the context's
+// gathers (row t) at the receiver row.  fields (host, 16*X*Z, or null): the
+// final state; `theta_src` is the source sample theta carries at the source
+// cell in the last step (0 backward).
+int fo_run(ouc_ctx* ctx, const ouc_shot* shot, bool backward, float theta_src, float* fields) {
+    int rc;
     const size_t C = (size_t)ctx->X * ctx->Z;
-    if (cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
-        return fail(ctx, OUC_ECUDA, "wavelet upload failed");
+    if (!ctx->fo_sq) {
+        if (cudaMalloc(&ctx->fo_sq, 2 * ctx->fstride * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->fo_sq = nullptr;
+            return fail(ctx, OUC_ENOMEM, "cannot allocate the first-order model squares");
+        }
+        ctx->bytes += 2 * ctx->fstride * sizeof(float);
+    }
+    // raw field bases (guards included) of Vp, Vs (model fields 6, 7) and the squares
+    fo::k_squares<<<4 * 148, 256, 0, ctx->stream>>>(ctx->model + 6 * ctx->fstride, ctx->model + 7 * ctx->fstride,
+                                                    ctx->fo_sq, ctx->fo_sq + ctx->fstride, ctx->fstride);
+    ctx->timing.kernel_launches += 1;
     if ((rc = zero_side(ctx, 1, 0, false))) return rc;
-    // state on the source side's 24 fields: velocities now[4] / past[4],
-    // stresses fo[4] + o[0..3] / fn[4] + o[4..7]
     const Side& s = ctx->src0;
     const float* vA[4] = {s.now[0], s.now[1], s.now[2], s.now[3]};
     float* vB[4] = {s.past[0], s.past[1], s.past[2], s.past[3]};
@@ -262,33 +330,37 @@ int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, flo
     float* sB[8] = {s.fn[0], s.fn[1], s.fn[2], s.fn[3], s.o[4], s.o[5], s.o[6], s.o[7]};
     fo::FoArgs a;
     memset(&a, 0, sizeof(a));
-    a.X = ctx->X; a.Z = ctx->Z; a.pitch = ctx->pitch; a.tiles_z = ctx->tiles_z; a.nt = ctx->nt;
+    a.X = ctx->X; a.Z = ctx->Z; a.pitch = ctx->pitch; a.tiles_z = ctx->tiles_z; a.nt = ctx->nt; a.L = ctx->L;
     a.sx = shot->sx + ctx->L; a.sz = shot->sz + ctx->L; a.rz = shot->rz + ctx->L;
     for (int k = 0; k < 6; ++k) a.a[k] = ctx->N == 6 ? fo::kFoWeights6[k] : ctx->a[k];
     a.dx = ctx->cfg.dx; a.dz = ctx->cfg.dz; a.dt = ctx->cfg.dt;
     a.rdx = 1.0f / ctx->cfg.dx; a.rdz = 1.0f / ctx->cfg.dz;
-    a.vp = ctx->vpv; a.vs = ctx->vsv; a.ax = ctx->ax; a.az = ctx->az;
-    a.wavelet = ctx->d_wavelet;
+    a.vp2 = ctx->field(ctx->fo_sq, 0); a.vs2 = ctx->field(ctx->fo_sq, 1); a.ax = ctx->ax; a.az = ctx->az;
+    a.wavelet = backward ? nullptr : ctx->d_wavelet;
     float* gx = ctx->gather(0, 0);
     float* gz = ctx->gather(0, 1);
     cudaEventRecord(ctx->ev[1], ctx->stream);
-    for (int t = 0; t < ctx->nt; ++t) {
-        const bool even = (t & 1) == 0;
+    for (int n = 0; n < ctx->nt; ++n) {
+        const int t = backward ? ctx->nt - 1 - n : n;
+        const bool even = (n & 1) == 0;
         for (int k = 0; k < 4; ++k) { a.vold[k] = even ? vA[k] : vB[k]; a.vnew[k] = even ? vB[k] : (float*)vA[k]; }
         for (int k = 0; k < 8; ++k) { a.sold[k] = even ? sA[k] : sB[k]; a.snew[k] = even ? sB[k] : sA[k]; }
         a.t = t;
-        a.rec_x = gx + (size_t)t * ctx->X;
-        a.rec_z = gz + (size_t)t * ctx->X;
+        if (backward) {
+            a.inj_x = gx + (size_t)t * ctx->X;
+            a.inj_z = gz + (size_t)t * ctx->X;
+        } else {
+            a.rec_x = gx + (size_t)t * ctx->X;
+            a.rec_z = gz + (size_t)t * ctx->X;
+        }
         if (ctx->N == 2) fo::launch<2>(a, ctx->tiles_x, ctx->stream);
         else if (ctx->N == 5) fo::launch<5>(a, ctx->tiles_x, ctx->stream);
         else fo::launch<6>(a, ctx->tiles_x, ctx->stream);
         ctx->timing.kernel_launches += 1;
     }
     cudaEventRecord(ctx->ev[2], ctx->stream);
-    if (gather_vx && (rc = gather_out(ctx, gx, gather_vx, true))) return rc;
-    if (gather_vz && (rc = gather_out(ctx, gz, gather_vz, true))) return rc;
     if (fields) {
-        // the newest level: written by step nt-1
+        // the newest level: written by the last step
         const bool last_even = ((ctx->nt - 1) & 1) == 0;
         const float* v[4];
         const float* st[8];
@@ -296,9 +368,9 @@ int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, flo
         for (int k = 0; k < 8; ++k) st[k] = last_even ? sB[k] : sA[k];
         // 16 host fields: Vx Vz Vpx Vpz Vsx Vsz theta omega Qzx Qzz Qxx Qxz theta_x theta_z omega_x omega_z
         const float* order[12] = {v[0], v[1], v[2], v[3], st[6], st[7], st[4], st[5], st[0], st[1], st[2], st[3]};
+        const int dst[12] = {2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15};
         for (int k = 0; k < 12; k += 4) {
             launch_pack_fields(order + k, 4, ctx->X, ctx->Z, ctx->pitch, ctx->staging, ctx->stream);
-            const int dst[12] = {2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15};
             for (int q = 0; q < 4; ++q)
                 if (cudaMemcpyAsync(fields + (size_t)dst[k + q] * C, ctx->staging + (size_t)q * C, C * 4,
                                     cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
@@ -307,21 +379,55 @@ int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, flo
         }
     }
     const cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "first-order forward");
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "first-order time loop");
     if (fields) {
-        // totals as the kernels form them: U = P + S, theta = theta_x + theta_z + s
-        // (s the last wavelet sample at the source cell), omega = omega_x + omega_z
+        // totals as the kernels form them: U = P + S, theta = theta_x + theta_z + s,
+        // omega = omega_x + omega_z
         const size_t src_cell = (size_t)(shot->sx + ctx->L) * ctx->Z + (shot->sz + ctx->L);
         for (size_t k = 0; k < C; ++k) {
-            const float s = k == src_cell ? wavelet[ctx->nt - 1] : 0.0f;
+            const float sv = k == src_cell ? theta_src : 0.0f;
             fields[k] = fields[2 * C + k] + fields[4 * C + k];
             fields[C + k] = fields[3 * C + k] + fields[5 * C + k];
-            fields[6 * C + k] = fields[12 * C + k] + fields[13 * C + k] + s;
+            fields[6 * C + k] = fields[12 * C + k] + fields[13 * C + k] + sv;
             fields[7 * C + k] = fields[14 * C + k] + fields[15 * C + k];
         }
     }
-    ctx->timing.forward_ms = elapsed(ctx->ev[1], ctx->ev[2]);
+    (backward ? ctx->timing.backward_ms : ctx->timing.forward_ms) = elapsed(ctx->ev[1], ctx->ev[2]);
     return OUC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ouc_forward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet, float* gather_vx, float* gather_vz,
+                   float* fields) {
+    int rc = fo_check(ctx, shot);
+    if (rc) return rc;
+    if (!wavelet) return fail(ctx, OUC_EINVAL, "wavelet is NULL");
+    cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;
+    ctx->timing = ouc_timing{};
+    if (cudaMemcpyAsync(ctx->d_wavelet, wavelet, (size_t)ctx->nt * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        return fail(ctx, OUC_ECUDA, "wavelet upload failed");
+    if ((rc = fo_run(ctx, shot, false, wavelet[ctx->nt - 1], fields))) return rc;
+    if (gather_vx && (rc = gather_out(ctx, ctx->gather(0, 0), gather_vx, true))) return rc;
+    if (gather_vz && (rc = gather_out(ctx, ctx->gather(0, 1), gather_vz, true))) return rc;
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "gather download");
+    return OUC_OK;
+}
+
+int ouc_backward_fo(ouc_ctx* ctx, const ouc_shot* shot, const float* rec_vx, const float* rec_vz, float* fields) {
+    int rc = fo_check(ctx, shot);
+    if (rc) return rc;
+    if (!rec_vx || !rec_vz) return fail(ctx, OUC_EINVAL, "records are NULL");
+    cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;
+    ctx->timing = ouc_timing{};
+    if ((rc = gather_in(ctx, rec_vx, ctx->gather(0, 0), true))) return rc;
+    if ((rc = gather_in(ctx, rec_vz, ctx->gather(0, 1), true))) return rc;
+    return fo_run(ctx, shot, true, 0.0f, fields);
 }
 
 }  // extern "C"

@@ -115,6 +115,62 @@ def test_first_order_error_vs_fp64_oracle(oracle, name):
     assert ours["gx"] < 1e-5 and ours["gz"] < 1e-5
 
 
+@pytest.mark.parametrize("name", ["g64n6", "g72x56n5", "c1"])
+@pytest.mark.parametrize("layout", [o.GATHER_XT, o.GATHER_TX])
+def test_first_order_backward_bit_exact_vs_reference_sm100(oracle, name, layout):
+    """Receiver back-propagation of the reference kernels' own records (the
+    *_backward_propagation kernels with load_record injection)."""
+    if not os.path.exists(os.path.join(REF_DIR, f"libpsref_cuda_{name}.so")):
+        pytest.skip("reference sm_100a build not present")
+    if name == "c1" and layout == o.GATHER_TX:
+        pytest.skip("one layout suffices at this size")
+    ref = RefBuild(name, "cuda")
+    vp, vs = _model(ref, 7)
+    pvp, pvs = _padded(ref, vp, vs)
+    ax, az = oracle.profile(pvp, ref.L)
+    w = _wavelet(ref.NT)
+    L = ref.L
+    sx, sz, rz = _shots(ref)[0]
+    args = (np.float32(6e-4), np.float32(8.0), np.float32(8.0), pvp, pvs, ax, az)
+    rx, rzz, _, _ = ref.forward_fo(sx + L, sz + L, rz + L, *args, w, ref.NT)
+    bf, _ = ref.backward_fo(rz + L, *args, rx, rzz, ref.NT)
+    with _context(ref, vp, vs, gather_layout=layout) as ctx:
+        recs = (rx, rzz) if layout == o.GATHER_XT else (rx.T, rzz.T)
+        f = ctx.backward_first_order(o.Shot(sx=sx, sz=sz, rz=rz), *recs)
+        t = ctx.timing()
+    assert np.abs(bf[0]).max() > 0
+    diff = {n: int(np.count_nonzero(f[k] != bf[k])) for k, n in enumerate(FIELDS)}
+    print(name, layout, "cells differing from the reference:", diff, "backward ms", t["backward_ms"])
+    assert not any(diff.values()), diff
+
+
+def test_first_order_throughput_c2(oracle):
+    """Cell-updates per second of the first-order forward loop on the
+    1000 x 500 interior (L = 30, N = 5, nt = 4000), ours against the
+    reference's stress + velocity kernels on the same GPU; the final state
+    must agree bit for bit."""
+    if not os.path.exists(os.path.join(REF_DIR, "libpsref_cuda_c2.so")):
+        pytest.skip("reference sm_100a build not present")
+    ref = RefBuild("c2", "cuda")
+    vp, vs = _model(ref, 9)
+    pvp, pvs = _padded(ref, vp, vs)
+    ax, az = oracle.profile(pvp, ref.L)
+    w = _wavelet(ref.NT)
+    L = ref.L
+    sx, sz, rz = (ref.X - 2 * L) // 2, 10, 5
+    cells = (ref.X - 2 * ref.N) * (ref.Z - 2 * ref.N) * ref.NT
+    with _context(ref, vp, vs) as ctx:
+        ctx.forward_first_order(o.Shot(sx=sx, sz=sz, rz=rz), w)   # warm-up
+        gx, gz, f = ctx.forward_first_order(o.Shot(sx=sx, sz=sz, rz=rz), w, fields=True)
+        ms = ctx.timing()["forward_ms"]
+    rx, rzz, rf, rms = ref.forward_fo(sx + L, sz + L, rz + L, np.float32(6e-4), np.float32(8.0), np.float32(8.0),
+                                      pvp, pvs, ax, az, w, ref.NT)
+    print(f"first-order forward c2: ours {ms:.1f} ms = {cells / ms / 1e6:.2f} Gcell/s; "
+          f"reference kernels {rms:.1f} ms = {cells / rms / 1e6:.2f} Gcell/s")
+    assert np.array_equal(gx, rx) and np.array_equal(gz, rzz)
+    assert all(np.array_equal(f[k], rf[k]) for k in range(16))
+
+
 def test_first_order_rejects_unsupported_forms():
     ref_like = type("R", (), dict(X=64, Z=64, L=12, N=6, NT=50))
     vp, vs = _model(ref_like, 1)

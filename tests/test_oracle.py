@@ -106,6 +106,16 @@ def test_first_order_oracle_bit_exact_vs_reference_kernels(oracle, name):
     dx_, dz_, df = oracle.forward_fo(sh, vp, vs, ax, az, src, fp64=True)
     assert rel_l2(rx, dx_) < 1e-5
 
+    # receiver back-propagation of these records (load_record injection,
+    # stress_backward_propagation, velocity_backward_propagation)
+    bf, _ = ref.backward_fo(sh.rz, np.float32(6e-4), np.float32(8.0), np.float32(8.0), vp, vs, ax, az, rx, rz, NT)
+    of = oracle.backward_fo(sh, vp, vs, ax, az, rx, rz)
+    assert np.abs(bf[0]).max() > 0
+    for k in range(16):
+        assert np.array_equal(bf[k], of[k]), k
+    df = oracle.backward_fo(sh, vp, vs, ax, az, rx, rz, fp64=True)
+    assert rel_l2(bf[2], df[2]) < 1e-4
+
 
 def test_padding_matches_reference(oracle):
     """orc_pad_model restates xiangbian (PS:37-119); compare with the fixture's padded model."""
