@@ -266,15 +266,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
     }
 }
 
+// The shared-memory opt-in is a per-device attribute: set on the current
+// device before every loop (fo_run), not once per process.
+template <int N>
+cudaError_t configure() {
+    return cudaFuncSetAttribute(k_fo<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, TileGeo<N>::bytes);
+}
+
 template <int N>
 void launch(const FoArgs& a, int tiles_x, cudaStream_t s) {
-    constexpr int bytes = TileGeo<N>::bytes;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_fo<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        configured = true;
-    }
-    k_fo<N><<<tiles_x * a.tiles_z, kThreads, bytes, s>>>(a);
+    k_fo<N><<<tiles_x * a.tiles_z, kThreads, TileGeo<N>::bytes, s>>>(a);
 }
 
 // Five-digit weights of the reference's first-order kernels (PS:405,
@@ -322,6 +323,8 @@ int fo_run(ouc_ctx* ctx, const ouc_shot* shot, bool backward, float theta_src, f
     fo::k_squares<<<4 * 148, 256, 0, ctx->stream>>>(ctx->model + 6 * ctx->fstride, ctx->model + 7 * ctx->fstride,
                                                     ctx->fo_sq, ctx->fo_sq + ctx->fstride, ctx->fstride);
     ctx->timing.kernel_launches += 1;
+    const cudaError_t ce = ctx->N == 2 ? fo::configure<2>() : ctx->N == 5 ? fo::configure<5>() : fo::configure<6>();
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "first-order kernel configuration");
     if ((rc = zero_side(ctx, 1, 0, false))) return rc;
     const Side& s = ctx->src0;
     const float* vA[4] = {s.now[0], s.now[1], s.now[2], s.now[3]};
@@ -359,6 +362,8 @@ int fo_run(ouc_ctx* ctx, const ouc_shot* shot, bool backward, float theta_src, f
         ctx->timing.kernel_launches += 1;
     }
     cudaEventRecord(ctx->ev[2], ctx->stream);
+    const cudaError_t le = cudaGetLastError();   // launch-configuration errors are not reported by the sync
+    if (le != cudaSuccess) return cuda_fail(ctx, le, "first-order step launch");
     if (fields) {
         // the newest level: written by the last step
         const bool last_even = ((ctx->nt - 1) & 1) == 0;
