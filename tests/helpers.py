@@ -19,6 +19,21 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
 
 
+def worst(errors):
+    """Largest error of a dict of errors; a NaN error counts as infinite (a
+    plain max() would skip it depending on the order)."""
+    v = [float(x) for x in errors.values()]
+    return float("inf") if any(np.isnan(x) for x in v) else max(v)
+
+
+def finite_rel_l2(a, b):
+    """rel_l2 over the cells finite in both; the NaN/Inf cells must coincide
+    (0/0 image cells where the illumination is zero, as the reference gives)."""
+    fa, fb = np.isfinite(a), np.isfinite(b)
+    assert np.array_equal(fa, fb), "non-finite cells differ"
+    return rel_l2(np.asarray(a)[fa], np.asarray(b)[fb])
+
+
 def shot_cfg(g):
     from oracle.oracle import Shot
     return Shot(X=int(g["X"]), Z=int(g["Z"]), L=int(g["L"]), N=int(g["N"]), nt=int(g["NT"]), sx=int(g["sx"]),

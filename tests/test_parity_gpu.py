@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 import ouc_b200 as o
-from helpers import CASES, golden_shot, load_golden, make_context, rel_l2, shot_cfg
+from helpers import CASES, finite_rel_l2, golden_shot, load_golden, make_context, rel_l2, shot_cfg, worst
 from oracle.oracle import REF_DIR, RefBuild
 
 pytestmark = pytest.mark.gpu
@@ -38,8 +38,8 @@ def test_forward_matches_reference(name):
     eg = {"gx": rel_l2(gx, g["fwd_gx"]), "gz": rel_l2(gz, g["fwd_gz"])}
     ef = {n: rel_l2(f[k], g["fwd_fields"][k]) for k, n in enumerate(("Ux", "Uz", "Px", "Pz", "Sx", "Sz"))}
     print(name, eg, ef)
-    assert max(eg.values()) <= TOL_GATHER, eg
-    assert max(ef.values()) <= TOL_FIELD, ef
+    assert worst(eg) <= TOL_GATHER, eg
+    assert worst(ef) <= TOL_FIELD, ef
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -64,9 +64,9 @@ def test_rtm_matches_reference(name):
     with make_context(g) as ctx:
         pp, ps = ctx.rtm_shot(golden_shot(g), g["src"])
         spp, sps, sil = ctx.stack()
-    errs = {"lap_pp": rel_l2(pp, g["rtm_lap_pp"]), "lap_ps": rel_l2(ps, g["rtm_lap_ps"])}
+    errs = {"lap_pp": finite_rel_l2(pp, g["rtm_lap_pp"]), "lap_ps": finite_rel_l2(ps, g["rtm_lap_ps"])}
     print(name, errs)
-    assert max(errs.values()) <= TOL_IMAGE, errs
+    assert worst(errs) <= TOL_IMAGE, errs
     assert np.allclose(spp, pp.astype(np.float64)) and np.allclose(sps, ps.astype(np.float64))
     L, X, Z = int(g["L"]), int(g["X"]), int(g["Z"])
     assert rel_l2(sil, g["rtm_acc"][2][L:X - L, L:Z - L]) < TOL_FIELD
@@ -112,28 +112,29 @@ def test_matches_reference_cuda_kernels_on_b200(name):
     _, _, rfm, _ = ref.forward(sx, sz, rz, dt, dx, dx, g["vp"], g["vs"], g["ax"], g["az"], g["src"], nm)
     with make_context(g, nt=nm) as ctx:
         _, _, fm = ctx.forward(golden_shot(g), g["src"][:nm], fields=True)
-    e = {"gx": rel_l2(gx, rgx), "gz": rel_l2(gz, rgz), "lap_pp": rel_l2(pp, r["lap_pp"]),
-         "lap_ps": rel_l2(ps, r["lap_ps"])}
+    e = {"gx": rel_l2(gx, rgx), "gz": rel_l2(gz, rgz), "lap_pp": finite_rel_l2(pp, r["lap_pp"]),
+         "lap_ps": finite_rel_l2(ps, r["lap_ps"])}
     for k, n in enumerate(("Ux", "Uz", "Px", "Pz", "Sx", "Sz")):
         e[n] = rel_l2(f[k], rf[k])
         e[n + "_mid"] = rel_l2(fm[k], rfm[k])
     bitexact = {k: bool(np.array_equal(a, b)) for k, a, b in
                 (("gx", gx, rgx), ("fields", f[2:6], rf[2:6]), ("lap_pp", pp, r["lap_pp"]))}
     print(name, "vs reference CUDA", e, bitexact)
-    assert max(e.values()) <= TOL_REF, e
+    assert worst(e) <= TOL_REF, e
 
 
-@pytest.mark.parametrize("name", ["c1", "c2"])
+@pytest.mark.parametrize("name", ["c1", "c2", "c4s"])
 def test_workload_grids_match_reference_cuda_kernels(name):
     """Workload-size grids (many tiles in both directions, interior tiles,
     long runs): gathers and the RTM images against the reference's sm_100a
-    kernels on the same model and shot."""
+    kernels on the same model and shot.  c4s is the largest grid (4000 x 1500
+    interior, 4060 x 1560 padded) over its first 2000 steps."""
     from ouc_b200 import models
     lib = os.path.join(REF_DIR, f"libpsref_cuda_{name}.so")
     if not os.path.exists(lib):
         pytest.skip("reference sm_100a build not present")
     from oracle.oracle import Oracle
-    w = models.c1() if name == "c1" else models.c2()
+    w = {"c1": models.c1, "c2": models.c2, "c4s": lambda: models.c4(nt=2000)}[name]()
     cfg = w.cfg
     vp, vs = (w.vp, w.vs) if w.vp_mig is None else (w.vp_mig, w.vs_mig)
     L = cfg.npml
@@ -142,7 +143,7 @@ def test_workload_grids_match_reference_cuda_kernels(name):
     vsp = orc.pad(np.pad(vs, L), L)
     ax, az = orc.profile(vpp, L)
     wav, t0 = o.ricker(w.fm, cfg.dt, cfg.nt)
-    sh = w.shots[0]
+    sh = w.shots[len(w.shots) // 2 if name == "c4s" else 0]
     shot = o.Shot(sh.sx, sh.sz, sh.rz, t0=t0)
     ref = RefBuild(name, "cuda")
     f32 = np.float32
@@ -152,10 +153,14 @@ def test_workload_grids_match_reference_cuda_kernels(name):
     with o.Context(cfg, vp, vs) as ctx:
         gx, gz, _ = ctx.forward(shot, wav)
         pp, ps = ctx.rtm_shot(shot, wav)
-    e = {"gx": rel_l2(gx, rgx), "gz": rel_l2(gz, rgz), "lap_pp": rel_l2(pp, r["lap_pp"]),
-         "lap_ps": rel_l2(ps, r["lap_ps"])}
-    print(name, "vs reference CUDA", e, "bit-exact gathers:", bool(np.array_equal(gx, rgx)))
-    assert max(e.values()) <= TOL_REF, e
+    e = {"gx": rel_l2(gx, rgx), "gz": rel_l2(gz, rgz), "lap_pp": finite_rel_l2(pp, r["lap_pp"]),
+         "lap_ps": finite_rel_l2(ps, r["lap_ps"])}
+    finite = float(np.isfinite(pp).mean())
+    print(name, "vs reference CUDA", e, "bit-exact gathers:", bool(np.array_equal(gx, rgx)),
+          "bit-exact images:", bool(np.array_equal(pp, r["lap_pp"], equal_nan=True)),
+          f"finite image cells {finite:.3f}")
+    assert finite > (0.05 if name == "c4s" else 0.5)
+    assert worst(e) <= TOL_REF, e
 
 
 def test_batched_shots_equal_single_shots():

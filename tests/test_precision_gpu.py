@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import ouc_b200 as o
-from helpers import load_golden, make_context, golden_shot, rel_l2
+from helpers import load_golden, make_context, golden_shot, rel_l2, worst
 
 pytestmark = pytest.mark.gpu
 
@@ -115,7 +115,7 @@ def test_snapshot_form_vs_fp64_oracle(c1_fp64, K, prec, comp):
     print(f"snapshots every {K}, storage {prec}, compensated {comp}: vs FP64 {e}, below row {ACQ_ROWS} {ed}, "
           f"illumination {e_il:.2e}, device bytes {nbytes / 2**20:.1f} MiB")
     assert np.isfinite(pp).all() and np.isfinite(ps).all()
-    assert max(ed.values()) <= TOL_PRECISION, ed
+    assert worst(ed) <= TOL_PRECISION, ed
     if prec != o.PREC_BF16:
         assert e["pp"] <= TOL_PRECISION and e["ps"] <= 2 * TOL_PRECISION, e
     assert e_il <= TOL_PRECISION
