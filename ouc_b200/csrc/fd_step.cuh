@@ -498,6 +498,14 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
         constexpr int P2R = 2;
 #pragma unroll 1
         for (int q0 = 0; q0 < 4; q0 += P2R) {
+        // the model's operands first: their latency runs under the derivatives
+        float4 vp2r[P2R], vs2r[P2R];
+#pragma unroll
+        for (int qq = 0; qq < P2R; ++qq) {
+            const ptrdiff_t g = (ptrdiff_t)(x0 + r0 + q0 + qq) * P + (z0 + c);
+            vp2r[qq] = ld4(gm.vp2 + g);
+            vs2r[qq] = ld4(gm.vs2 + g);
+        }
         float4 exx[P2R], ezx[P2R];
         dx4<N, P2R, false>(ux0 + q0 * UC, UC, a, dvx, exx);   // dvxdx = D-x Ux
         dx4<N, P2R, true>(uz0 + q0 * UC, UC, a, dvx, ezx);    // dvzdx = D+x Uz
@@ -510,7 +518,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
             const float4 exz = dz4<N, true>(ux0 + q * UC, a, dvz);    // dvxdz = D+z Ux
             const float4 ezz = dz4<N, false>(uz0 + q * UC, a, dvz);   // dvzdz = D-z Uz
             const ptrdiff_t g = (ptrdiff_t)gi * P + gjb;
-            const float4 vp2 = ld4(gm.vp2 + g), vs2 = ld4(gm.vs2 + g);
+            const float4 vp2 = vp2r[qq], vs2 = vs2r[qq];
             const bool own = ownc && r >= 0 && r < TX;
             float4 fxx = zero4(), fzz = zero4(), fxz = zero4(), fzx = zero4();
             if (f.px) {
@@ -632,13 +640,18 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
 #pragma unroll 1
         for (int q = 0; q < 2; ++q) {
             const int r = rr + q;
+            const int gi = x0 + r;
+            const ptrdiff_t g = (ptrdiff_t)gi * P + (z0 + c);
+            // the leapfrog's operands first: their latency runs under the derivatives
+            const float4 npx = ld4(nowp[0] + g), npz = ld4(nowp[1] + g);
+            const float4 nsx = ld4(nowp[2] + g), nsz = ld4(nowp[3] + g);
+            const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);
+            const float4 osx = ld4(p.past[2] + off + g), osz = ld4(p.past[3] + off + g);
             float4 tx[1], wx[1], dB[1], dE[1];
             dx4<N, 1, true>(sTh + (r + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
             dx4<N, 1, false>(sOm + (r + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
             dx4<N, 1, false>(sQxz + (r + SHX) * TZ + c, TZ, a, dvx, dB);     // dux_zdx = D-x Qxz
             dx4<N, 1, true>(sQzz + (r + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
-            const int gi = x0 + r;
-            const ptrdiff_t g = (ptrdiff_t)gi * P + (z0 + c);
             const float4 tz = dz4<N, true>(sTh + (r + SHX) * SC + scol, a, dvz);    // dthetadz
             const float4 wz = dz4<N, false>(sOm + (r + SHX) * SC + scol, a, dvz);   // domegadz
             const float4 dA = dz4<N, true>(sQxx + r * SC + scol, a, dvz);           // dux_xdz = D+z Qxx
@@ -671,10 +684,6 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
                 spx = mul4(spx, bxv); ssx = mul4(ssx, bxv);
                 spz = mul4(spz, bzv); ssz = mul4(ssz, bzv);
             }
-            const float4 npx = ld4(nowp[0] + g), npz = ld4(nowp[1] + g);
-            const float4 nsx = ld4(nowp[2] + g), nsz = ld4(nowp[3] + g);
-            const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);
-            const float4 osx = ld4(p.past[2] + off + g), osz = ld4(p.past[3] + off + g);
             const float2 two = dup2(2.f), dt2 = dup2(p.dt2), m1 = dup2(-1.f);
             auto leap = [&](float4 now, float4 past, float4 sum) {
                 return cat4(fma2(dt2, lo2(sum), fma2(two, lo2(now), mul2(lo2(past), m1))),
