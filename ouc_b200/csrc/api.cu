@@ -10,6 +10,8 @@
 // other, PS:2108).
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -700,6 +702,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->Xc = ctx->tiles_x * TX; ctx->Zc = ctx->tiles_z * TZ;
     ctx->pitch = ((kZOFF + ctx->Zc + kZOFF) + 31) / 32 * 32;
     ctx->fstride = (size_t)(ctx->Xc + 2 * kGX) * ctx->pitch;
+    if (ctx->fstride > (size_t)INT_MAX) return bad("grid too large: one field would exceed 2^31 cells", OUC_EINVAL);
     ctx->shot_stride = (size_t)kFieldsPerShot * ctx->fstride;
     ctx->rec_tx0 = L / TX; ctx->rec_tz0 = L / TZ;
     ctx->rec_tiles_x = (X - L - 1) / TX - ctx->rec_tx0 + 1;

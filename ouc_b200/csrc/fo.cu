@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
     // ---- phase 1: U = P + S velocity over the tile and a 2N halo ----------
     for (int idx = tid; idx < G::UR * (UC / 4); idx += kThreads) {
         const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
-        const ptrdiff_t g = (ptrdiff_t)(ux_i0 + r) * P + (ux_j0 + 4 * c4);
+        const int g = (ux_i0 + r) * P + (ux_j0 + 4 * c4);
         float4 ux = add4(ld4(p.vold[0] + g), ld4(p.vold[2] + g));   // Vx = Vpx + Vsx
         float4 uz = add4(ld4(p.vold[1] + g), ld4(p.vold[3] + g));
         const int gi = ux_i0 + r, gj = ux_j0 + 4 * c4;
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
             const int r = r0 + q, gi = x0 + r, gjb = z0 + c;
             const float4 exz = dz4<N, true>(ux0 + q * UC, a, dvz);    // dvxdz = D+z Vx
             const float4 ezz = dz4<N, false>(uz0 + q * UC, a, dvz);   // dvzdz = D-z Vz
-            const ptrdiff_t g = (ptrdiff_t)gi * P + gjb;
+            const int g = gi * P + gjb;
             const float4 vp2v = ld4(p.vp2 + g), vs2v = ld4(p.vs2 + g), axv = ld4(p.ax + g), azv = ld4(p.az + g);
             float4 so[8], sn[8];
 #pragma unroll
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
             const float4 wzv = dz4<N, false>(sOm + (r + SHX) * SC + scol, a, dvz);  // domegadz
             const float4 dA = dz4<N, true>(sQxx + r * SC + scol, a, dvz);           // dux_xdz = D+z Qxx
             const float4 dC = dz4<N, false>(sQzx + r * SC + scol, a, dvz);          // duz_xdz = D-z Qzx
-            const ptrdiff_t g = (ptrdiff_t)gi * P + (z0 + c);
+            const int g = gi * P + (z0 + c);
             const float4 axv = ld4(p.ax + g), azv = ld4(p.az + g);
             const float4 opx = ld4(p.vold[0] + g), opz = ld4(p.vold[1] + g);
             const float4 osx = ld4(p.vold[2] + g), osz = ld4(p.vold[3] + g);
