@@ -96,8 +96,8 @@ int ouc_forward_learned(ouc_ctx* ctx, ouc_cnn* net, const ouc_shot* shot, const 
 /* Fine forward modeling sampled as the coarse grid sees it: gathers of the
  * restricted displacement (cubic midpoint interpolation along the staggered
  * direction) at the coarse receiver row, every second fine step; (X/2) x
- * nt_coarse each in the fine context's gather layout.  The judge of the
- * learned path. */
+ * nt_coarse each in the fine context's gather layout.  The spot check of
+ * the learned path compares against these. */
 int ouc_forward_restricted(ouc_ctx* fine, const ouc_shot* shot, const float* wavelet, int nt_coarse,
                            float* gather_vx, float* gather_vz);
 

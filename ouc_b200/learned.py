@@ -1,12 +1,12 @@
 """The learned coarse path (include/ouc_corrector.h): a half-order-2 run at
 twice the spacing and time step, corrected every few steps by a small CNN
 trained on fine/coarse pairs that the method itself generates; the fine
-half-order-5 run is the judge (sparse spot-check traces) and the fallback.
+half-order-5 run is the referee (sparse spot-check traces) and the fallback.
 
 ``Twin`` holds a fine context and its coarse twin on one model; ``pairs``
 generates training data on the GPU, ``train`` fits the network (tensor-core
 kernels, Adam), ``model_shots`` runs a survey of shots on the coarse path with
-the spot-check judge and the fine-grid fallback.
+the spot check and the fine-grid fallback.
 """
 from __future__ import annotations
 
@@ -121,7 +121,7 @@ class Twin:
         return gx, gz
 
     def fine_forward_restricted(self, shot: Shot, w_fine):
-        """The fine run's gathers as the coarse grid sees them (the judge)."""
+        """The fine run's gathers as the coarse grid sees them (the referee)."""
         cfg = self.coarse_cfg
         gx = np.zeros(self._gshape(self.coarse.X, cfg.nt, self.fine_cfg), np.float32)
         gz = np.zeros_like(gx)

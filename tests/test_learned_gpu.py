@@ -1,6 +1,6 @@
 """The learned coarse path: half-order 2 at twice the spacing and time step,
 corrected every 8 steps by the CNN trained on the GPU on fine/coarse pairs
-the method generates; the fine half-order-5 run is the judge.
+the method generates; the fine half-order-5 run is the referee.
 
 Workload: fine 2 m / 0.2 ms, 256 x 192 interior + 20-cell CPML (coarse 4 m /
 0.4 ms, 128 x 96 + 10), 30 Hz Ricker, seeded random flat-layer models with
@@ -48,7 +48,7 @@ def misfit(g, ref, shot):
 
 
 def test_restricted_gathers_sample_the_fine_state():
-    """The judge's gathers equal the 4-point midpoint restriction of the fine
+    """The referee's gathers equal the 4-point midpoint restriction of the fine
     run's own displacement (numpy, from the final fields of the same run)."""
     vp, vs = model(5)
     w, _ = o.ricker(FM, DT, NT)
@@ -139,7 +139,7 @@ def test_trained_corrector_against_the_plain_coarse_run(trained):
     because the weight-gradient sums are accumulated in no fixed order: at
     30 Hz on 4 m the coarse method's own error over one 8-step interval is
     small, and the network's residual on held-out states is larger than what
-    it corrects.  The spot-check judge below is what keeps such shots out of
+    it corrects.  The spot check below is what keeps such shots out of
     the delivered results."""
     net, _, _ = trained
     w, _ = o.ricker(FM, DT, NT)
@@ -157,7 +157,7 @@ def test_trained_corrector_against_the_plain_coarse_run(trained):
     assert np.all(np.isfinite(corr))
 
 
-def test_spot_check_judge_and_fallback(trained):
+def test_spot_check_and_fallback(trained):
     """Checked shots above the tolerance are replaced by the fine run, and so
     are the unchecked shots after them; below it the coarse result stands."""
     net, _, _ = trained

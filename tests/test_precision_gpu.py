@@ -104,7 +104,7 @@ def test_snapshot_form_vs_fp64_oracle(c1_fp64, K, prec, comp):
     """The precision form: source snapshots every K imaging levels (scaled
     FP16 or BF16) instead of the backward reconstruction, compensated
     imaging sums, FP64 stack.  The stored forward field is what an exact
-    reconstruction returns, so the judge is the FP64 oracle with exact strip
+    reconstruction returns, so the reference point is the FP64 oracle with exact strip
     restore.  Bounds: PP and PS within 1 % below the acquisition zone; over
     the whole image PP within 1 % and PS within 2 % (the plain FP32 method's
     whole-image errors, printed above, are larger)."""
