@@ -597,6 +597,13 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     if (cfg->dx > 256.f || cfg->dz > 256.f) return bad("grid spacing above 256 is not supported");
     if (!(cfg->pml_r > 0 && cfg->pml_r < 1)) return bad("pml_r must be in (0, 1)");
     if (cfg->max_batch < 0 || cfg->max_batch > 256) return bad("max_batch must be in [0, 256]");
+    {   // one field (guard rows and columns, padded to whole tiles) must stay
+        // below 2^31 cells: the kernels address within a field with 32-bit offsets
+        const long long Xp = (long long)cfg->nx + 2LL * L, Zp = (long long)cfg->nz + 2LL * L;
+        const long long rows = (Xp + 31) / 32 * 32 + 2LL * kGX;
+        const long long pitch = ((Zp + 63) / 64 * 64 + 2LL * kZOFF + 31) / 32 * 32;
+        if (rows * pitch > (long long)INT_MAX) return bad("grid too large: one field would exceed 2^31 cells");
+    }
     if (cfg->strip_precision != OUC_PREC_FP32 && cfg->strip_precision != OUC_PREC_FP16 &&
         cfg->strip_precision != OUC_PREC_BF16)
         return bad("strip_precision must be OUC_PREC_FP32, OUC_PREC_FP16 or OUC_PREC_BF16");
@@ -701,8 +708,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->tiles_x = (X + TX - 1) / TX; ctx->tiles_z = (Z + TZ - 1) / TZ;
     ctx->Xc = ctx->tiles_x * TX; ctx->Zc = ctx->tiles_z * TZ;
     ctx->pitch = ((kZOFF + ctx->Zc + kZOFF) + 31) / 32 * 32;
-    ctx->fstride = (size_t)(ctx->Xc + 2 * kGX) * ctx->pitch;
-    if (ctx->fstride > (size_t)INT_MAX) return bad("grid too large: one field would exceed 2^31 cells", OUC_EINVAL);
+    ctx->fstride = (size_t)(ctx->Xc + 2 * kGX) * ctx->pitch;   // < 2^31 (checked above)
     ctx->shot_stride = (size_t)kFieldsPerShot * ctx->fstride;
     ctx->rec_tx0 = L / TX; ctx->rec_tz0 = L / TZ;
     ctx->rec_tiles_x = (X - L - 1) / TX - ctx->rec_tx0 + 1;

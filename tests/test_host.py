@@ -82,3 +82,34 @@ def test_create_rejects_bad_configs_without_touching_the_device():
         with pytest.raises(o.OucError) as e:
             o.Context(o.Config(**base, **bad_cfg), vp, vs)
         assert e.value.code == 1
+
+
+def test_create_rejects_grids_beyond_32bit_field_offsets():
+    """The kernels address within one field with 32-bit offsets, so a grid
+    whose padded field would exceed 2^31 cells is refused before the model is
+    read or the device touched.  Called through the C ABI with a dummy model
+    (the Python wrapper would first want a model of that size), in a child
+    process, so that a missing check fails this test instead of the run."""
+    import subprocess
+    import sys
+
+    def field_cells(nx, nz, L):   # rows and pitch of one padded field
+        X, Z = nx + 2 * L, nz + 2 * L
+        rows = -(-X // 32) * 32 + 32
+        pitch = -(-(-(-Z // 64) * 64 + 32) // 32) * 32
+        return rows * pitch
+
+    for nx, nz in ((50000, 50000), (200000, 12000)):
+        assert field_cells(nx, nz, 20) > 2**31 - 1
+        code = f"""
+import ctypes as C, numpy as np, ouc_b200 as o
+small = np.full(16, 3000, np.float32)
+p = small.ctypes.data_as(C.POINTER(C.c_float))
+h = C.c_void_p()
+cfg = o.Config(nx={nx}, nz={nz}, npml=20, dx=10.0, dz=10.0, dt=1e-3, nt=10, half_order=5)
+print(o.lib().ouc_create(C.byref(cfg.c()), p, p, None, C.byref(h)), bool(h.value))
+"""
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120,
+                           cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+        assert r.returncode == 0, r.stderr[-2000:]
+        assert r.stdout.split() == ["1", "False"], r.stdout
