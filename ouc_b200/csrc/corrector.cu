@@ -298,11 +298,9 @@ __global__ void __launch_bounds__(kThreadsConv) k_conv5(const ConvArgs a) {
 template <int CIN, int COUT, int EPI>
 void launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
     constexpr int bytes = ConvGeo<CIN, COUT>::bytes;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_conv5<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        configured = true;
-    }
+    // the shared-memory opt-in is a per-device setting: set on the current
+    // device at every launch (a host-side call; a few launches per step)
+    cudaFuncSetAttribute(k_conv5<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     const int tiles = a.n * a.H * ((a.W + kTile - 1) / kTile);
     const int grid = tiles < 2 * sms ? tiles : 2 * sms;
     k_conv5<CIN, COUT, EPI><<<grid, kThreadsConv, bytes, s>>>(a);

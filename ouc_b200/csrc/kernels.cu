@@ -24,8 +24,9 @@ static void configure_modes() {
     configure_one<N, kRec>();
 }
 
-// Shared-memory attributes of the step kernels of half-order N, set once per
-// process (and per device the caller makes current) before their first launch.
+// Shared-memory attributes of the step kernels of half-order N on the current
+// device (a per-device setting): ouc_create sets them for its device, the
+// no-allocation entry point at its set-up on each device.
 void configure_step_kernels(int N) {
     if (N == 2) configure_modes<2>();
     if (N == 5) configure_modes<5>();
@@ -35,11 +36,6 @@ void configure_step_kernels(int N) {
 template <int N, int MODE>
 static void launch_one(const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
     constexpr int bytes = TileGeo<N>::bytes;
-    static bool configured = false;   // one attribute call per instantiation (callers outside a context)
-    if (!configured) {
-        configure_one<N, MODE>();
-        configured = true;
-    }
     k_step<N, MODE><<<dim3(tiles_x * a.tiles_z, nshots), kThreads, bytes, s>>>(a);
 }
 

@@ -110,6 +110,9 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     if (!g_scratch_addr[dev]) {
         float* ptr = nullptr;
         if (cudaGetSymbolAddress((void**)&ptr, g_scratch) != cudaSuccess || !ptr) return OUC_ECUDA;
+        // the step kernels' shared-memory opt-in is a per-device setting too
+        for (int n : {2, 5, 6}) configure_step_kernels(n);
+        if (cudaGetLastError() != cudaSuccess) return OUC_ECUDA;
         g_scratch_addr[dev] = ptr;
     }
     float* base = g_scratch_addr[dev];
