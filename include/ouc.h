@@ -312,7 +312,8 @@ int ouc_set_run_batch(ouc_ctx* ctx, int n);
  * d_vp, d_vs padded X*Z models (x-major), d_wavelet nt samples, gathers X*nt
  * each in cfg->gather_layout.  Work is queued on cfg->stream and the call
  * returns without synchronising.  The first call on a device looks up the
- * array's address: make it before any stream capture on that device.  All
+ * array's address and sets the kernels' shared-memory limit there: make it
+ * before any stream capture on that device.  All
  * calls share the array and it keeps the last call's contents (each call
  * clears what it needs zeroed); calls whose work overlaps on the GPU race, so
  * serialise them.  Sizes beyond the array return OUC_ESCRATCH; the CFL check

@@ -17,8 +17,9 @@
 //     module loading, from the first call on that GPU), held until the
 //     process exits;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) -- make that first call before any stream
-//     capture on that device;
+//     (cudaGetSymbolAddress) and sets the step kernels' shared-memory limit
+//     on that device -- make that first call before any stream capture on
+//     that device;
 //   * all calls share the one array and it keeps the previous call's
 //     contents: every call clears what must start at zero, and calls whose
 //     work overlaps on the GPU (different streams, or different host
