@@ -67,7 +67,7 @@ enum { OUC_GATHER_XT = 0, OUC_GATHER_TX = 1 };
 typedef struct ouc_config {
     int nx, nz;             /* interior grid                                     */
     int npml;               /* absorbing width L in cells (PS:15)                */
-    int half_order;         /* stencil half-width N: 2..6 (PS:16 uses 6)          */
+    int half_order;         /* stencil half-width N: 2, 5 or 6 (PS:16 uses 6)    */
     float dx, dz, dt;       /* spacing (m) and time step (s)                     */
     int nt;                 /* time steps per shot (PS:17)                       */
     double pml_r;           /* target reflection R of the damping profile (PS:23)  */
