@@ -363,6 +363,14 @@ def main():
     tr = committed_traffic()
     traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name and tr.get("batch") == B else None
 
+    # saved source wavefield per shot: 8 ring fields per step (strip form) or
+    # the two P components of every K-th imaging level (snapshot form)
+    elem = 4 if args.strips == "fp32" else 2
+    if args.snapshot_every:
+        saved, saved_what = -(-nt // args.snapshot_every) * 2 * cfg.nx * cfg.nz * elem, "source snapshots"
+    else:
+        saved, saved_what = (nt - 1) * 8 * ring_cells(cfg) * elem, "boundary strips"
+
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
@@ -377,7 +385,7 @@ def main():
                        "strips": args.strips, "compensated_image": bool(args.compensated),
                        "source_wavefield": (f"snapshots every {args.snapshot_every} imaging levels" if args.snapshot_every
                                             else "reconstructed from boundary strips"),
-                       "l2": "256 MiB buffer written between timed shots; 3.8 GB of boundary strips per shot",
+                       "l2": f"256 MiB buffer written between timed shots; {saved / 1e9:.1f} GB of {saved_what} per shot",
                        "parallelism": f"shots sharded over {world} GPU(s)"},
             "shots_per_hour": shots_per_hour,
             "phase_ms": {"forward": statistics.median(fwd_ms), "backward": statistics.median(bwd_ms)},
