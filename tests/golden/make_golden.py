@@ -55,11 +55,21 @@ def make(name):
     nt_mid = NT // 2
     _, _, f, _ = ref.forward(sx, sz, rz, np.float32(dt), np.float32(dx), np.float32(dx), vp, vs, ax, az, src, nt_mid)
     r = ref.rtm(sx, sz, rz, t0, np.float32(dt), np.float32(dx), np.float32(dx), vp, vs, ax, az, src)
+    # first-order velocity-stress kernels (stress/velocity and their
+    # backward-propagation twins): gathers, the 12 state fields at mid-run
+    # (Vpx Vpz Vsx Vsz, the four Q fields, theta_x theta_z omega_x omega_z)
+    # and the state after back-propagating the gathers
+    args = (np.float32(dt), np.float32(dx), np.float32(dx), vp, vs, ax, az)
+    fo_gx, fo_gz, _, _ = ref.forward_fo(sx, sz, rz, *args, src, NT)
+    _, _, fo_f, _ = ref.forward_fo(sx, sz, rz, *args, src, nt_mid)
+    fo_b, _ = ref.backward_fo(rz, *args, fo_gx, fo_gz, NT)
+    fo_state = [2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15]
     out = dict(X=X, Z=Z, L=L, N=N, NT=NT, nt_mid=nt_mid, fm=fm, dt=dt, dx=dx, sx=sx, sz=sz, rz=rz, t0=t0,
                vp=vp, vs=vs, ax=ax, az=az, src=src,
                fwd_gx=gx, fwd_gz=gz, fwd_fields=f[:6],
                rtm_lap_pp=r["lap_pp"], rtm_lap_ps=r["lap_ps"], rtm_acc=r["acc"], rtm_rec=r["rec"],
-               rtm_fields=r["fields"][:6])
+               rtm_fields=r["fields"][:6],
+               fo_gx=fo_gx, fo_gz=fo_gz, fo_fields=fo_f[fo_state], fo_bwd_fields=fo_b[fo_state])
     path = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path))

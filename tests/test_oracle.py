@@ -117,6 +117,30 @@ def test_first_order_oracle_bit_exact_vs_reference_kernels(oracle, name):
     assert rel_l2(bf[2], df[2]) < 1e-4
 
 
+FO_STATE = [2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15]   # Vpx..Vsz, the Q fields, theta_x..omega_z
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_first_order_oracle_matches_golden(oracle, name):
+    """The oracle's first-order restatement against the fixtures of the
+    reference's stress/velocity kernels (and their backward-propagation twins)
+    run on the CPU: bit-exact gathers, mid-run state and back-propagated
+    state.  Needs no reference sources."""
+    g = load_golden(name)
+    sh = shot_cfg(g)
+    gx, gz, _ = oracle.forward_fo(sh, g["vp"], g["vs"], g["ax"], g["az"], g["src"])
+    assert np.abs(g["fo_gx"]).max() > 0
+    assert np.array_equal(gx, g["fo_gx"]) and np.array_equal(gz, g["fo_gz"])
+    sh_mid = shot_cfg(g)
+    sh_mid.nt = int(g["nt_mid"])
+    _, _, f = oracle.forward_fo(sh_mid, g["vp"], g["vs"], g["ax"], g["az"], g["src"][: sh_mid.nt])
+    for k, i in enumerate(FO_STATE):
+        assert np.array_equal(f[i], g["fo_fields"][k]), i
+    b = oracle.backward_fo(sh, g["vp"], g["vs"], g["ax"], g["az"], g["fo_gx"], g["fo_gz"])
+    for k, i in enumerate(FO_STATE):
+        assert np.array_equal(b[i], g["fo_bwd_fields"][k]), i
+
+
 def test_padding_matches_reference(oracle):
     """orc_pad_model restates xiangbian (PS:37-119); compare with the fixture's padded model."""
     g = load_golden("g72x56n5")
