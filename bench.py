@@ -127,10 +127,9 @@ def cpu_sample(steps_hint=None, threads=None, budget_s=12.0):
     vp = orc.pad(np.pad(w.vp_mig, L), L)
     vs = orc.pad(np.pad(w.vs_mig, L), L)
     ax, az = orc.profile(vp, L)
-    from ouc_b200 import ricker
     nts = steps_hint or 8
     while True:
-        src, t0 = ricker(w.fm, cfg.dt, nts)
+        src, t0 = orc.ricker(w.fm, cfg.dt, nts)   # the oracle's restatement: this arm never maps libouc.so
         sh = Shot(X=X, Z=Z, L=L, N=cfg.half_order, nt=nts, sx=L + w.shots[0].sx, sz=L + 2, rz=L + 2, dx=cfg.dx,
                   dz=cfg.dz, dt=cfg.dt, t0=t0)
         t1 = time.perf_counter()

@@ -310,7 +310,11 @@ int ouc_set_run_batch(ouc_ctx* ctx, int n);
  * array of OUC_NOALLOC_SCRATCH_BYTES (held on each GPU that loads it until
  * process exit).  Inputs and outputs are the caller's device buffers:
  * d_vp, d_vs padded X*Z models (x-major), d_wavelet nt samples, gathers X*nt
- * each in cfg->gather_layout.  Work is queued on cfg->stream and the call
+ * each in cfg->gather_layout.  cfg->model_layout must be OUC_MODEL_PADDED and
+ * cfg->density 0 (density-normalised equations only); other values return
+ * OUC_EINVAL before any device work.  A CUDA error already pending on the
+ * calling thread returns OUC_ECUDA and is left for its owner to read.  Work
+ * is queued on cfg->stream and the call
  * returns without synchronising.  The first call on a device looks up the
  * array's address and sets the kernels' shared-memory limit there: make it
  * before any stream capture on that device.  All

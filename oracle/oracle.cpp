@@ -46,6 +46,7 @@ typedef struct orc_cfg {
     int src_in_recon;  // 1 (exact mode): add the source term inside the reconstruction
     float dx, dz, dt, dh;
     float coeff[8];    // a_1..a_N (PS:221 for N=6)
+    int src_type;      // 0: theta source (PS:331-338, 380); 1: vertical force on Uz (no reference counterpart)
 } orc_cfg;
 }
 
@@ -435,10 +436,26 @@ struct Engine {
         }
     }
 
+    // Vertical-force source (src_type 1, the extension of the library's
+    // OUC_SRC_FORCE_Z; the reference only injects into theta, PS:380):
+    // dt^2 w[t] is added to the P part of Uz at the source cell after the
+    // leapfrog, and U = P + S there is formed again.  In float the sum is one
+    // fused multiply-add, as the CUDA kernels compile it.
+    void force(Wave<T>& w, const float* src, int t) {
+        const int i = cfg.sx, j = cfg.sz;
+        const T dt2 = dt * dt;
+        T& pz = w.pnz(i, j);
+        if (sizeof(T) == sizeof(float)) pz = (T)std::fma((float)dt2, (float)src[t], (float)pz);
+        else pz = pz + dt2 * (T)src[t];
+        w.uz(i, j) = pz + w.snz(i, j);
+    }
+
     void forward(Wave<T>& w, const float* src, T* rvx, T* rvz, StripStore<T>* st, const Bands* b) {
+        const bool theta = cfg.src_type == 0;
         for (int t = 0; t < cfg.nt; ++t) {
-            stage_s(w, t, src, true);
+            stage_s(w, t, src, theta);
             stage_u(w);
+            if (!theta) force(w, src, t);
             if (rvx) record(w, rvx, rvz, t);
             if (st && t != cfg.nt - 1) save_bands(w, *b, *st, t);
         }
@@ -857,5 +874,24 @@ void orc_cpml_profile(const float* vp, int X, int Z, int L, double R, float* ax,
 
 int orc_num_threads(void) { return omp_get_max_threads(); }
 void orc_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
+
+// Ricker wavelet as the reference's main() builds it (PS:1954-1958):
+// Nk = PI^2 FM^2 dt^2 formed in double from PI = 3.1415926 (PS:14) and
+// stored as float, t0 = ceil(1 / (FM dt)) samples, the exponent taken in
+// float, the product in double and stored as float.
+int orc_ricker(float fm, float dt, int nt, float* out, int* t0_out) {
+    if (!(fm > 0) || !(dt > 0) || nt < 1 || !out) return 1;
+    const double pi_ref = 3.1415926;
+    const double f = fm;
+    const float nk = (float)(pi_ref * pi_ref * f * f * dt * dt);
+    const int t0 = (int)ceil(1.0 / (f * dt));
+    for (int t = 0; t < nt; ++t) {
+        const int d = t - t0;
+        const float e = std::exp(-nk * d * d);
+        out[t] = (float)((1.0 - 2.0 * nk * d * d) * e);
+    }
+    if (t0_out) *t0_out = t0;
+    return 0;
+}
 
 }  // extern "C"

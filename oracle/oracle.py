@@ -33,7 +33,7 @@ class OrcCfg(C.Structure):
                 ("strip_level", C.c_int), ("image_align", C.c_int), ("do_mute", C.c_int),
                 ("src_in_recon", C.c_int),
                 ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("dh", C.c_float),
-                ("coeff", C.c_float * 8)]
+                ("coeff", C.c_float * 8), ("src_type", C.c_int)]
 
 
 def _ptr(a, kind=np.float32):
@@ -79,11 +79,12 @@ class Shot:
     image_align: int = 0
     do_mute: int = 1
     src_in_recon: int = 0
+    src_type: int = 0      # 0: theta source (the reference's); 1: vertical force on Uz
 
     def cfg(self) -> OrcCfg:
         c = OrcCfg()
         for k in ("X", "Z", "L", "N", "nt", "sx", "sz", "rz", "t0", "strip_level", "image_align", "do_mute",
-                  "src_in_recon"):
+                  "src_in_recon", "src_type"):
             setattr(c, k, int(getattr(self, k)))
         c.dx, c.dz, c.dt, c.dh = self.dx, self.dz, self.dt, self.dx
         w = weights(self.N)
@@ -126,12 +127,22 @@ class Oracle:
         self.lib.orc_pad_model.argtypes = [_fp, C.c_int, C.c_int, C.c_int]
         self.lib.orc_cpml_profile.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_double, _fp, _fp]
         self.lib.orc_num_threads.restype = C.c_int
+        self.lib.orc_ricker.argtypes = [C.c_float, C.c_float, C.c_int, _fp, C.POINTER(C.c_int)]
+        self.lib.orc_ricker.restype = C.c_int
         self.lib.orc_set_threads.argtypes = [C.c_int]
 
     def threads(self, n=None):
         if n:
             self.lib.orc_set_threads(int(n))
         return self.lib.orc_num_threads()
+
+    def ricker(self, fm, dt, nt):
+        """Ricker wavelet of the reference's main() (PS:1954-1958) and its delay t0."""
+        out = np.zeros(nt, np.float32)
+        t0 = C.c_int()
+        if self.lib.orc_ricker(fm, dt, nt, _ptr(out), C.byref(t0)):
+            raise ValueError("bad Ricker parameters")
+        return out, t0.value
 
     def pad(self, a, L):
         a = np.ascontiguousarray(a, dtype=np.float32).copy()

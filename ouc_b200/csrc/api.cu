@@ -30,22 +30,6 @@ static_assert((int)OUC_PREC_FP32 == (int)ouc::kStripF32 && (int)OUC_PREC_FP16 ==
                   (int)OUC_PREC_BF16 == (int)ouc::kStripBF16,
               "strip precision codes");
 
-namespace {
-
-// Float32 staggered weights.  N = 6: the reference's literals (PS:221).
-// Other N: the exact Taylor solution of sum_k c_k (2k-1)^(2n-1) = [n==1],
-// rounded to float32.
-const double kWeights[7][6] = {
-    {0, 0, 0, 0, 0, 0},
-    {1.0, 0, 0, 0, 0, 0},
-    {1.125, -1.0 / 24.0, 0, 0, 0, 0},
-    {75.0 / 64.0, -25.0 / 384.0, 3.0 / 640.0, 0, 0, 0},
-    {1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0, 0, 0},
-    {19845.0 / 16384.0, -735.0 / 8192.0, 567.0 / 40960.0, -405.0 / 229376.0, 35.0 / 294912.0, 0},
-    {1.2213364, -9.6931458e-2, 1.7447662e-2, -2.9672895e-3, 3.5900540e-4, -2.1847812e-5},
-};
-
-}  // namespace
 
 
 namespace ouc {
@@ -556,7 +540,7 @@ int ouc_version(void) { return OUC_VERSION_MAJOR * 100 + OUC_VERSION_MINOR; }
 
 int ouc_stencil_weights(int half_order, float* out) {
     if (half_order < 1 || half_order > 6 || !out) return OUC_EINVAL;
-    for (int k = 0; k < half_order; ++k) out[k] = (float)kWeights[half_order][k];
+    for (int k = 0; k < half_order; ++k) out[k] = (float)kStencilWeights[half_order][k];
     return OUC_OK;
 }
 
@@ -617,7 +601,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     ctx->X = cfg->nx + 2 * L; ctx->Z = cfg->nz + 2 * L;
     ctx->batch = std::max(1, cfg->max_batch);
     ctx->run_batch = ctx->batch;
-    for (int k = 0; k < N; ++k) ctx->a[k] = (float)kWeights[N][k];
+    for (int k = 0; k < N; ++k) ctx->a[k] = (float)kStencilWeights[N][k];
     const int X = ctx->X, Z = ctx->Z;
 
     // model on the padded grid
@@ -643,7 +627,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         if (!(v >= 0) || !std::isfinite(v)) return bad("Vs must be non-negative and finite");
     // stability of the staggered leapfrog: dt vmax sum|a_k| sqrt(1/dx^2 + 1/dz^2) <= 1
     double sa = 0;
-    for (int k = 0; k < N; ++k) sa += fabs(kWeights[N][k]);
+    for (int k = 0; k < N; ++k) sa += fabs(kStencilWeights[N][k]);
     const double cfl = cfg->dt * vmax * sa * sqrt(1.0 / (cfg->dx * cfg->dx) + 1.0 / (cfg->dz * cfg->dz));
     if (cfl > 1.0) return bad("CFL number " + std::to_string(cfl) + " > 1 for this dt", OUC_EUNSTABLE);
     std::vector<float> hax((size_t)X * Z), haz((size_t)X * Z);

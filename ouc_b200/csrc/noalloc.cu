@@ -79,15 +79,10 @@ __global__ void k_model(const ModelArgs m) {
     }
 }
 
-const double kWeightsNoalloc[7][6] = {
-    {0, 0, 0, 0, 0, 0},
-    {1.0, 0, 0, 0, 0, 0},
-    {1.125, -1.0 / 24.0, 0, 0, 0, 0},
-    {75.0 / 64.0, -25.0 / 384.0, 3.0 / 640.0, 0, 0, 0},
-    {1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0, 0, 0},
-    {19845.0 / 16384.0, -735.0 / 8192.0, 567.0 / 40960.0, -405.0 / 229376.0, 35.0 / 294912.0, 0},
-    {1.2213364, -9.6931458e-2, 1.7447662e-2, -2.9672895e-3, 3.5900540e-4, -2.1847812e-5},
-};
+// The shot descriptor is written by the device from a by-value kernel
+// argument, so the call queues only kernels, memsets and device-to-device
+// copies (no host-to-device copy from pageable memory).
+__global__ void k_put_desc(ShotDesc* dst, const ShotDesc desc) { *dst = desc; }
 
 }  // namespace
 
@@ -97,13 +92,26 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     if (!cfg || !shot || !d_vp || !d_vs || !d_wavelet || !d_gather_vx || !d_gather_vz) return OUC_EINVAL;
     const int N = cfg->half_order, L = cfg->npml;
     if (N != 2 && N != 5 && N != 6) return OUC_EINVAL;
+    // this entry point reads a padded X x Z model, runs the density-normalised
+    // equations and writes one of the two gather layouts; anything else is
+    // refused before any device work
+    if (cfg->model_layout != OUC_MODEL_PADDED || cfg->density != 0) return OUC_EINVAL;
+    if (cfg->gather_layout != OUC_GATHER_XT && cfg->gather_layout != OUC_GATHER_TX) return OUC_EINVAL;
     if (cfg->nx < 4 * N || cfg->nz < 4 * N || L < N || L > kMaxPml || cfg->nt < 2) return OUC_EINVAL;
+    // sizes in 64-bit before any derived extent: X, Z and the pitch stay far
+    // below INT_MAX for every grid that can fit the array
+    if ((long long)cfg->nx + 2LL * L > (1LL << 24) || (long long)cfg->nz + 2LL * L > (1LL << 24) ||
+        (long long)cfg->nt > (1LL << 30))
+        return OUC_ESCRATCH;
     if (!(cfg->dx > 0) || !(cfg->dz > 0) || !(cfg->dt > 0) || cfg->dx > 256.f || cfg->dz > 256.f) return OUC_EINVAL;
     if (!(cfg->pml_r > 0 && cfg->pml_r < 1)) return OUC_EINVAL;
     if (shot->sx < 0 || shot->sx >= cfg->nx || shot->sz < 0 || shot->sz >= cfg->nz || shot->rz < 0 ||
         shot->rz >= cfg->nz || (shot->src_type != OUC_SRC_THETA && shot->src_type != OUC_SRC_FORCE_Z))
         return OUC_EINVAL;
     cudaStream_t stream = (cudaStream_t)cfg->stream;
+    // an error left by the caller's own earlier work is theirs to read: report
+    // it without clearing it, before queueing anything
+    if (cudaPeekAtLastError() != cudaSuccess) return OUC_ECUDA;
 
     // set-up, once per device: the array's device address
     int dev = 0;
@@ -162,13 +170,13 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     desc.strip_slot = 0;
     desc.vp2 = field(0); desc.vs2 = field(1); desc.ax = field(2); desc.az = field(3);
     desc.bx = nullptr; desc.bz = nullptr;   // density-normalised equations only
-    if (cudaMemcpyAsync(d_desc, &desc, sizeof(desc), cudaMemcpyHostToDevice, stream) != cudaSuccess) return OUC_ECUDA;
+    k_put_desc<<<1, 1, 0, stream>>>(d_desc, desc);
 
     StepArgs a;
     memset(&a, 0, sizeof(a));
     a.X = X; a.Z = Z; a.pitch = pitch; a.L = L;
     a.tiles_z = tiles_z;
-    for (int k = 0; k < N; ++k) a.a[k] = (float)kWeightsNoalloc[N][k];
+    for (int k = 0; k < N; ++k) a.a[k] = (float)kStencilWeights[N][k];
     a.dx = cfg->dx; a.dz = cfg->dz; a.dt = cfg->dt; a.dt2 = cfg->dt * cfg->dt;
     a.rdx = 1.0f / cfg->dx; a.rdz = 1.0f / cfg->dz;
     a.vp2 = field(0); a.vs2 = field(1); a.ax = field(2); a.az = field(3);

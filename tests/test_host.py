@@ -58,6 +58,15 @@ def test_ricker_matches_reference_construction():
     assert w[t0] == 1.0
 
 
+@pytest.mark.parametrize("fm,dt,nt", [(30.0, 1e-3, 240), (25.0, 5e-4, 4000), (20.0, 1e-3, 1000), (30.0, 4e-4, 600)])
+def test_oracle_ricker_equals_the_library_bit_for_bit(oracle, fm, dt, nt):
+    # the CPU baseline builds its wavelet with the oracle's restatement
+    w, t0 = o.ricker(fm, dt, nt)
+    wo, t0o = oracle.ricker(fm, dt, nt)
+    assert t0 == t0o
+    assert np.array_equal(w, wo)
+
+
 def test_create_rejects_bad_configs_without_touching_the_device():
     vp = np.full((64, 64), 3000, np.float32)
     vs = np.full((64, 64), 1700, np.float32)
