@@ -182,3 +182,21 @@ def test_stencil_weights_taylor_conditions():
 def test_layered_model_shape():
     vp, vs = layered_model(40, 32, 6)
     assert vp.shape == (40, 32) and vs.min() > 0
+
+
+def test_oracle_force_source_float_and_double_agree(oracle):
+    """The vertical-force source (an extension without a reference
+    counterpart): the float and double instantiations agree to FP32
+    round-off, and the force run differs from the theta-source run."""
+    g = load_golden("g72x56n5")
+    sh = shot_cfg(g)
+    sh.src_type = 1
+    fx32, fz32, f32 = oracle.forward(sh, g["vp"], g["vs"], g["ax"], g["az"], g["src"])
+    fx64, fz64, f64 = oracle.forward(sh, g["vp"], g["vs"], g["ax"], g["az"], g["src"], fp64=True)
+    assert rel_l2(fx32, fx64) < 1e-5 and rel_l2(fz32, fz64) < 1e-5
+    # separated P/S fields carry FP32 cancellation (about 5e-4 here; U is 5e-6)
+    assert max(rel_l2(f32[k], f64[k]) for k in range(2)) < 1e-5
+    assert max(rel_l2(f32[k], f64[k]) for k in range(2, 6)) < 2e-3
+    sh.src_type = 0
+    tx, tz, _ = oracle.forward(sh, g["vp"], g["vs"], g["ax"], g["az"], g["src"])
+    assert rel_l2(fz32, tz) > 0.5

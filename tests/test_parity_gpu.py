@@ -11,6 +11,7 @@ Tolerances (relative L2 per field):
     fields and ~1e-3 for the images -> 1e-5, 5e-4 and 3e-3;
   * against the FP64 oracle: asserted at the same floors and printed.
 """
+import dataclasses
 import os
 
 import numpy as np
@@ -126,9 +127,13 @@ def test_matches_reference_cuda_kernels_on_b200(name):
 @pytest.mark.parametrize("name", ["c1", "c2", "c4s"])
 def test_workload_grids_match_reference_cuda_kernels(name):
     """Workload-size grids (many tiles in both directions, interior tiles,
-    long runs): gathers and the RTM images against the reference's sm_100a
-    kernels on the same model and shot.  c4s is the largest grid (4000 x 1500
-    interior, 4060 x 1560 padded) over its first 2000 steps."""
+    long runs): gathers, the six displacement fields (U, P, S; after nt steps
+    and at mid-run) and the RTM images against the reference's sm_100a
+    kernels on the same model and shot, at 1e-5 relative L2 per field; the
+    gathers and fields are also asserted bit-identical (the kernels reproduce
+    every rounding of the reference's compiled expressions).  c4s is the
+    largest grid (4000 x 1500 interior, 4060 x 1560 padded) over its first
+    2000 steps."""
     from ouc_b200 import models
     lib = os.path.join(REF_DIR, f"libpsref_cuda_{name}.so")
     if not os.path.exists(lib):
@@ -147,20 +152,33 @@ def test_workload_grids_match_reference_cuda_kernels(name):
     shot = o.Shot(sh.sx, sh.sz, sh.rz, t0=t0)
     ref = RefBuild(name, "cuda")
     f32 = np.float32
-    rgx, rgz, _, _ = ref.forward(L + sh.sx, L + sh.sz, L + sh.rz, f32(cfg.dt), f32(cfg.dx), f32(cfg.dz), vpp, vsp, ax,
-                                 az, wav, cfg.nt)
+    fargs = (L + sh.sx, L + sh.sz, L + sh.rz, f32(cfg.dt), f32(cfg.dx), f32(cfg.dz), vpp, vsp, ax, az, wav)
+    rgx, rgz, rf, _ = ref.forward(*fargs, cfg.nt)
+    nm = cfg.nt // 2
+    _, _, rfm, _ = ref.forward(*fargs, nm)
     r = ref.rtm(L + sh.sx, L + sh.sz, L + sh.rz, t0, f32(cfg.dt), f32(cfg.dx), f32(cfg.dz), vpp, vsp, ax, az, wav)
     with o.Context(cfg, vp, vs) as ctx:
-        gx, gz, _ = ctx.forward(shot, wav)
+        gx, gz, f = ctx.forward(shot, wav, fields=True)
         pp, ps = ctx.rtm_shot(shot, wav)
+    cm = dataclasses.replace(cfg, nt=nm)
+    with o.Context(cm, vp, vs) as ctx:
+        _, _, fm = ctx.forward(shot, wav[:nm], fields=True)
     e = {"gx": rel_l2(gx, rgx), "gz": rel_l2(gz, rgz), "lap_pp": finite_rel_l2(pp, r["lap_pp"]),
          "lap_ps": finite_rel_l2(ps, r["lap_ps"])}
+    names = ("Ux", "Uz", "Px", "Pz", "Sx", "Sz")
+    for k, n in enumerate(names):
+        e[n] = rel_l2(f[k], rf[k])
+        e[n + "_mid"] = rel_l2(fm[k], rfm[k])
+    bitexact = {"gathers": bool(np.array_equal(gx, rgx) and np.array_equal(gz, rgz)),
+                "fields": all(np.array_equal(f[k], rf[k]) for k in range(6)),
+                "fields_mid": all(np.array_equal(fm[k], rfm[k]) for k in range(6)),
+                "images": bool(np.array_equal(pp, r["lap_pp"], equal_nan=True)
+                               and np.array_equal(ps, r["lap_ps"], equal_nan=True))}
     finite = float(np.isfinite(pp).mean())
-    print(name, "vs reference CUDA", e, "bit-exact gathers:", bool(np.array_equal(gx, rgx)),
-          "bit-exact images:", bool(np.array_equal(pp, r["lap_pp"], equal_nan=True)),
-          f"finite image cells {finite:.3f}")
+    print(name, "vs reference CUDA", e, "bit-exact:", bitexact, f"finite image cells {finite:.3f}")
     assert finite > (0.05 if name == "c4s" else 0.5)
     assert worst(e) <= TOL_REF, e
+    assert bitexact["gathers"] and bitexact["fields"] and bitexact["fields_mid"], bitexact
 
 
 def test_batched_shots_equal_single_shots():
