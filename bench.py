@@ -231,6 +231,20 @@ def run_survey(args, rank, world):
     return 0
 
 
+def relaunch(n):
+    """--gpus N > 1 without a launcher: run this script as N ranks (one
+    process per GPU) under torch.distributed.run on 127.0.0.1; rank 0 prints
+    the line.  An outer timeout bounds ranks that wait for one another."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "1800", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,9 +265,13 @@ def main():
                          "K: store source snapshots every K imaging levels instead (--strips sets their storage)")
     args = ap.parse_args()
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args.gpus)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if world != args.gpus and "WORLD_SIZE" in os.environ and args.gpus > 1:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload == "c3":
@@ -323,13 +341,14 @@ def main():
         bwd_ms.append(t["backward_ms"])
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev)
+    # the cross-shot exchange after the timed shots: sum of the ranks' FP64
+    # stacks (PP, PS, illumination); it also leaves the stack empty for e2e
+    from ouc_b200 import survey
+    stk = [torch.from_numpy(a).cuda() for a in mig.stack(reset=True)]
     if world > 1:
         tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-        # the cross-shot exchange: sum of the ranks' FP64 stacks (PP, PS, illumination)
-        from ouc_b200 import survey
-        stk = [torch.from_numpy(a).cuda() for a in mig.stack(reset=True)]
         survey.reduce_stack(*stk)
         dist.barrier()
     clk = clocks.stop()
@@ -339,14 +358,26 @@ def main():
     value = cells * args.steps * world / (ms / 1e3) / 1e9
     shots_per_hour = 3600.0 * B * args.steps * world / (ms / 1e3)
 
-    # e2e through the host API with pinned buffers
+    # e2e through the survey call a user makes (ouc_b200.survey.migrate):
+    # this rank's shots through the host API with pinned records in and
+    # images out, its FP64 stacks read back and summed over the ranks
     pin = [(torch.from_numpy(r[0]).pin_memory().numpy(), torch.from_numpy(r[1]).pin_memory().numpy()) for r in records]
+    all_shots = [None] * (B * world)
+    all_recs = [None] * (B * world)
+    for k in range(B):                       # round-robin: rank r migrates shots r, r + world, ...
+        all_shots[rank + k * world] = my_shots[k]
+        all_recs[rank + k * world] = pin[k]
+    for k in range(len(all_shots)):          # other ranks' slots: placeholders this rank never runs
+        if all_shots[k] is None:
+            all_shots[k] = my_shots[0]
     e2e_steps = max(2, args.steps // 2)
-    mig.rtm_batch(my_shots, wavelet, recs=pin)
+    survey.migrate(mig, all_shots, wavelet, recs=all_recs, rank=rank, world=world)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     t1 = time.perf_counter()
     for k in range(e2e_steps):
-        mig.rtm_batch(my_shots, wavelet, recs=pin)
+        survey.migrate(mig, all_shots, wavelet, recs=all_recs, rank=rank, world=world)
     e2e_s = time.perf_counter() - t1
     if world > 1:
         tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -388,8 +419,10 @@ def main():
                        "parallelism": f"shots sharded over {world} GPU(s)"},
             "shots_per_hour": shots_per_hour,
             "phase_ms": {"forward": statistics.median(fwd_ms), "backward": statistics.median(bwd_ms)},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * 2 * nt * X * 4 + nt * 4,
-                    "d2h_bytes_per_step": B * 2 * cfg.nx * cfg.nz * 4,
+            "e2e": {"value": e2e, "unit": UNIT, "call": "ouc_b200.survey.migrate (ouc_rtm_batch + ouc_stack + FP64 "
+                                                           "stack all-reduce)",
+                    "h2d_bytes_per_step": B * 2 * nt * X * 4 + nt * 4,
+                    "d2h_bytes_per_step": B * 2 * cfg.nx * cfg.nz * 4 + 3 * cfg.nx * cfg.nz * 8,
                     "shots_per_hour": 3600.0 * B * e2e_steps * world / e2e_s},
             "roofline": {"kernel": f"k_step<5, forward> (fused S+U stage, CPML, strip save), {B} shots per launch",
                          "bound": "hbm",

@@ -300,6 +300,17 @@ int ouc_survey_rtm(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_ap
 int ouc_tune_batch(ouc_ctx* ctx, int steps, int* best_batch, float* ns_per_cell);
 int ouc_set_run_batch(ouc_ctx* ctx, int n);
 
+/* Step-kernel geometry.  seg_rows > 0 (a multiple of 16): the x-marching
+ * kernel, each CTA walking a 64-column strip down a segment of that many rows
+ * in 16-row blocks with bulk asynchronous row copies; 0: one CTA per 32 x 64
+ * tile.  Both replace the reference's per-step kernel pair (forward_s +
+ * forward_u, PS:316-384 / PS:205-314, and their receiver and reconstruction
+ * twins) with bit-identical results.  ouc_create picks about 192 rows;
+ * ouc_tune_batch times the candidates.  Changing it drops the captured time
+ * loops (they are captured again on next use). */
+int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows);
+int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows);
+
 /* Forward modeling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they need
  * a modeling run: applications whose own memory pool owns the whole GPU and

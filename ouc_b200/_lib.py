@@ -52,6 +52,8 @@ SIGNATURES = {
     "ouc_create": (C.c_int, [C.POINTER(ouc_config), _fp, _fp, _fp, C.POINTER(_vp)]),
     "ouc_destroy": (C.c_int, [_vp]),
     "ouc_dims": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "ouc_set_step_kernel": (C.c_int, [_vp, C.c_int]),
+    "ouc_get_step_kernel": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "ouc_stream": (_vp, [_vp]),
     "ouc_last_timing": (C.c_int, [_vp, C.POINTER(ouc_timing)]),
     "ouc_device_bytes": (C.c_size_t, [_vp]),

@@ -366,6 +366,16 @@ class Context:
                                  int(reset)), self._h)
         return gp, gs, il
 
+    def set_step_kernel(self, seg_rows):
+        """Step-kernel geometry: x-marching segments of seg_rows rows (a
+        multiple of 16), or 0 for the 32 x 64 tile kernel (ouc_set_step_kernel)."""
+        check(lib().ouc_set_step_kernel(self._h, int(seg_rows)), self._h)
+
+    def step_kernel(self):
+        v = C.c_int()
+        check(lib().ouc_get_step_kernel(self._h, C.byref(v)), self._h)
+        return v.value
+
     def stack(self, reset=False):
         n = (self.cfg.nx, self.cfg.nz)
         pp, ps, il = np.zeros(n), np.zeros(n), np.zeros(n)

@@ -50,6 +50,28 @@ int cuda_fail(ouc_ctx* c, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);   \
     } while (0)
 
+// Read and clear the context's device status word after a synchronising call:
+// a bounded copy wait that gave up, or a non-finite wavefield.
+int check_status(ouc_ctx* ctx) {
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (st == 0) return OUC_OK;
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (st & 1) return fail(ctx, OUC_ETIMEOUT, "a step kernel's copy wait timed out");
+    return fail(ctx, OUC_EUNSTABLE, "non-finite wavefield (unstable run: check the CFL number and the inputs)");
+}
+
+// Rows per x-marching segment by default: about 192 (a multiple of 16), so
+// that a segment's S-stage halo (twice the stencil's row halo) stays a few
+// per cent of its work while a batch still spreads over several waves.
+int default_seg_rows(int X) {
+    const int nseg = std::max(1, (X + 191) / 192);
+    const int rows = (X + nseg - 1) / nseg;
+    return std::max(64, (rows + 15) / 16 * 16);
+}
+
 // Edge padding of the interior model into the absorbing layer, as the
 // reference's xiangbian (PS:37-119): sides copy the nearest interior
 // row/column, corners the nearest interior corner cell.
@@ -113,6 +135,8 @@ StepArgs base_args(const ouc_ctx* c) {
     a.strip_prec = c->cfg.strip_precision;
     a.comp_image = c->cfg.compensated_image;
     a.density = c->cfg.density;
+    a.seg_rows = c->seg_rows;
+    a.err = c->d_status;
     for (int k = 0; k < 3; ++k) a.comp[k] = c->comp[k];
     a.ring = c->ring;
     a.shots = c->d_desc;
@@ -467,6 +491,7 @@ int finalize(ouc_ctx* ctx, int n) {
         f.stack[k] = ctx->d_stack[k];
     }
     f.img = ctx->d_img;
+    f.status = ctx->d_status;
     launch_finalize(f, ctx->stream);
     ctx->timing.kernel_launches += 1;
     CK(cudaGetLastError());
@@ -535,6 +560,8 @@ const char* ouc_strerror(int status) {
 }
 
 const char* ouc_last_error(const ouc_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+
 
 int ouc_version(void) { return OUC_VERSION_MAJOR * 100 + OUC_VERSION_MINOR; }
 
@@ -726,6 +753,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
               cudaMalloc(&ctx->d_wavelet, (size_t)ctx->nt * 4) == cudaSuccess &&
               cudaMalloc(&ctx->d_img, 2 * ni * ctx->batch * 4) == cudaSuccess &&
               cudaMalloc(&ctx->d_desc, ctx->batch * sizeof(ShotDesc)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_status, sizeof(int)) == cudaSuccess &&
               cudaMalloc(&ctx->d_stack[0], ni * 8) == cudaSuccess && cudaMalloc(&ctx->d_stack[1], ni * 8) == cudaSuccess &&
               cudaMalloc(&ctx->d_stack[2], ni * 8) == cudaSuccess;
     if (!ok) {
@@ -737,6 +765,8 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     // guards and padding of every field must stay zero: clear everything once
     cudaMemsetAsync(ctx->model, 0, model_bytes, ctx->stream);
     cudaMemsetAsync(ctx->state, 0, state_bytes, ctx->stream);
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+    ctx->seg_rows = default_seg_rows(ctx->X);
     for (int q = 0; q < 3; ++q) cudaMemsetAsync(ctx->d_stack[q], 0, ni * 8, ctx->stream);
     ctx->vp2 = ctx->field(ctx->model, 0); ctx->vs2 = ctx->field(ctx->model, 1);
     ctx->ax = ctx->field(ctx->model, 2); ctx->az = ctx->field(ctx->model, 3);
@@ -755,7 +785,11 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     for (int q = 0; q < 3; ++q) ctx->comp[q] = ctx->field(ctx->state, k++);
     ctx->src0 = ctx->src;
     ctx->rcv0 = ctx->rcv;
-    configure_step_kernels(N);   // kernel attributes set before any graph capture
+    // kernel attributes set before any graph capture
+    if (configure_step_kernels(N) != cudaSuccess) {
+        cudaGetLastError();
+        return bad("cannot set the step kernels' shared-memory attributes", OUC_ECUDA);
+    }
     int rc = OUC_OK;
     if ((rc = upload_field(ctx, ctx->vp2, vp2.data())) || (rc = upload_field(ctx, ctx->vs2, vs2.data())) ||
         (rc = upload_field(ctx, ctx->ax, hax.data())) || (rc = upload_field(ctx, ctx->az, haz.data())) ||
@@ -775,7 +809,7 @@ int ouc_destroy(ouc_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->model); cudaFree(ctx->state);
     cudaFree(ctx->gathers); cudaFree(ctx->staging); cudaFree(ctx->d_wavelet);
-    cudaFree(ctx->d_img); cudaFree(ctx->d_desc);
+    cudaFree(ctx->d_img); cudaFree(ctx->d_desc); cudaFree(ctx->d_status);
     for (auto* p : ctx->d_stack) cudaFree(p);
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
@@ -786,6 +820,26 @@ int ouc_destroy(ouc_ctx* ctx) {
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+    return OUC_OK;
+}
+
+int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows) {
+    if (!ctx) return OUC_EINVAL;
+    if (seg_rows != 0 && (seg_rows < 16 || seg_rows % 16 != 0))
+        return fail(ctx, OUC_EINVAL, "segment rows must be 0 (tiles) or a positive multiple of 16");
+    if (seg_rows == ctx->seg_rows) return OUC_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    // captured time loops hold the old launch configuration
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+    ctx->graphs.clear();
+    ctx->seg_rows = seg_rows;
+    return OUC_OK;
+}
+
+int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows) {
+    if (!ctx || !seg_rows) return OUC_EINVAL;
+    *seg_rows = ctx->seg_rows;
     return OUC_OK;
 }
 
@@ -824,6 +878,10 @@ static int forward_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet
     if ((rc = upload_desc(ctx, 1, shot, d_w))) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     if ((rc = run_forward(ctx, 1, gx || gz, false))) return rc;
+    // runtime stability check: the recorded gathers (the receiver row of
+    // every step) and the final level must be finite
+    launch_finite_check(ctx->gather(0, 0), 2 * (size_t)ctx->nt * ctx->X, ctx->d_status, ctx->stream);
+    launch_finite_check(ctx->src.now[0] - (size_t)kGX * ctx->pitch - kZOFF, ctx->fstride, ctx->d_status, ctx->stream);
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     if (gx && (rc = gather_out(ctx, ctx->gather(0, 0), gx, host))) return rc;
     if (gz && (rc = gather_out(ctx, ctx->gather(0, 1), gz, host))) return rc;
@@ -835,6 +893,7 @@ static int forward_impl(ouc_ctx* ctx, const ouc_shot* shot, const float* wavelet
     }
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_status(ctx))) return rc;
     if (fields && host) {
         const size_t C = (size_t)ctx->X * ctx->Z;
         for (size_t k = 0; k < C; ++k) {
@@ -883,6 +942,12 @@ static int rtm_group(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_
         if ((shots[b].src_type == OUC_SRC_THETA) != theta) return fail(ctx, OUC_EINVAL, "mixed source types in a batch");
     rc = snap ? run_backward_snap(ctx, n) : run_backward(ctx, n, ctx->cfg.strip_level == OUC_STRIP_EXACT, theta);
     if (rc) return rc;
+    // runtime stability check: the modelled gathers and the imaging
+    // accumulators (source illumination and both correlations) must be finite
+    if (self_records) launch_finite_check(ctx->gather(0, 0), 2 * (size_t)ctx->nt * ctx->X * n, ctx->d_status, ctx->stream);
+    for (int b = 0; b < n; ++b)
+        launch_finite_check(ctx->acc[0] - (size_t)kGX * ctx->pitch - kZOFF + (size_t)b * ctx->shot_stride,
+                            3 * ctx->fstride, ctx->d_status, ctx->stream);
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     if ((rc = finalize(ctx, n))) return rc;
     if (ctx->cfg.gradient) {
@@ -904,6 +969,7 @@ static int rtm_group(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_
     }
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_status(ctx))) return rc;
     ctx->timing.forward_ms += elapsed(ctx->ev[0], ctx->ev[1]);
     ctx->timing.backward_ms += elapsed(ctx->ev[1], ctx->ev[2]);
     ctx->timing.finalize_ms += elapsed(ctx->ev[2], ctx->ev[3]);

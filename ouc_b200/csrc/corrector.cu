@@ -296,14 +296,18 @@ __global__ void __launch_bounds__(kThreadsConv) k_conv5(const ConvArgs a) {
 }
 
 template <int CIN, int COUT, int EPI>
-void launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
+cudaError_t launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
     constexpr int bytes = ConvGeo<CIN, COUT>::bytes;
     // the shared-memory opt-in is a per-device setting: set on the current
-    // device at every launch (a host-side call; a few launches per step)
-    cudaFuncSetAttribute(k_conv5<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    // device at every launch (a host-side call; a few launches per step);
+    // if it is refused nothing is launched and the caller reports it
+    const cudaError_t e = cudaFuncSetAttribute(k_conv5<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               bytes);
+    if (e != cudaSuccess) return e;
     const int tiles = a.n * a.H * ((a.W + kTile - 1) / kTile);
     const int grid = tiles < 2 * sms ? tiles : 2 * sms;
     k_conv5<CIN, COUT, EPI><<<grid, kThreadsConv, bytes, s>>>(a);
+    return cudaSuccess;
 }
 
 // ---- weight gradients (FP32), bias gradients, packing, Adam ---------------
@@ -578,14 +582,14 @@ int ouc_cnn_forward_dev(ouc_cnn* net, int n, int H, int W, const float* d_in, fl
     ConvArgs a{};
     a.n = n; a.H = H; a.W = W; a.err = net->err;
     a.x = net->x0; a.w = net->wf[0]; a.bias = net->params + p_offset(0) + w_count(0); a.y = net->y[0];
-    launch_conv<16, 32, kHidden>(a, net->sms, s);
+    if (launch_conv<16, 32, kHidden>(a, net->sms, s) != cudaSuccess) return OUC_ECUDA;
     for (int l = 1; l < 3; ++l) {
         a.x = net->y[l - 1]; a.w = net->wf[l]; a.bias = net->params + p_offset(l) + w_count(l); a.y = net->y[l];
-        launch_conv<32, 32, kHidden>(a, net->sms, s);
+        if (launch_conv<32, 32, kHidden>(a, net->sms, s) != cudaSuccess) return OUC_ECUDA;
     }
     a.x = net->y[2]; a.w = net->wf[3]; a.bias = net->params + p_offset(3) + w_count(3); a.y = d_out;
     a.cout_real = OUC_CNN_OUT;
-    launch_conv<32, 16, kOut>(a, net->sms, s);
+    if (launch_conv<32, 16, kOut>(a, net->sms, s) != cudaSuccess) return OUC_ECUDA;
     return cudaGetLastError() == cudaSuccess ? OUC_OK : OUC_ECUDA;
 }
 
@@ -606,14 +610,14 @@ int ouc_cnn_backward_dev(ouc_cnn* net, const float* d_gout, void* stream) {
     ConvArgs a{};
     a.n = n; a.H = H; a.W = W; a.err = net->err;
     a.x = net->g16; a.w = net->wd[3]; a.mask = net->y[2]; a.y = net->g[0];
-    launch_conv<16, 32, kDgrad>(a, net->sms, s);
+    if (launch_conv<16, 32, kDgrad>(a, net->sms, s) != cudaSuccess) return OUC_ECUDA;
     // layers 3 and 2
     for (int l = 2; l >= 1; --l) {
         const bf16* gl = net->g[(2 - l) & 1];
         k_wgrad<32, 32><<<wg, 256, 0, s>>>(n, H, W, net->y[l - 1], gl, kL[l].cin, kL[l].cout, gp + p_offset(l));
         k_bgrad<32><<<256, 256, 0, s>>>(P, gl, kL[l].cout, gp + p_offset(l) + w_count(l));
         a.x = gl; a.w = net->wd[l]; a.mask = net->y[l - 1]; a.y = net->g[(3 - l) & 1];
-        launch_conv<32, 32, kDgrad>(a, net->sms, s);
+        if (launch_conv<32, 32, kDgrad>(a, net->sms, s) != cudaSuccess) return OUC_ECUDA;
     }
     // layer 1
     const bf16* g1 = net->g[0];

@@ -39,6 +39,8 @@ struct ouc_ctx {
     int Xc = 0, Zc = 0, pitch = 0;
     int batch = 1;               // shots the device state holds (cfg.max_batch)
     int run_batch = 1;           // shots advanced per launch (<= batch; ouc_tune_batch)
+    int seg_rows = 0;            // step kernel: x-marching segments of this many rows, or 0 for 32 x 64 tiles
+    int* d_status = nullptr;     // device status word: bit 0 a copy wait timed out, bit 1 a non-finite field
     size_t fstride = 0;          // floats per field allocation
     size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;
@@ -138,6 +140,9 @@ int run_backward_snap_loop(ouc_ctx* ctx, int n);
 void damping(const std::vector<float>& vp, int X, int Z, int L, double R, std::vector<float>& ax,
              std::vector<float>& az);
 float elapsed(cudaEvent_t a, cudaEvent_t b);
+// Read and clear the device status word (after the stream's work): OUC_OK,
+// OUC_ETIMEOUT or OUC_EUNSTABLE.
+int check_status(ouc_ctx* ctx);
 
 }  // namespace host
 }  // namespace ouc

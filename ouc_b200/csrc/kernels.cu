@@ -5,36 +5,58 @@
 
 #include <algorithm>
 
+#include "fd_march.cuh"
 #include "fd_step.cuh"
 #include "ouc_internal.h"
 
 namespace ouc {
 
 template <int N, int MODE>
-static void configure_one() {
-    constexpr int bytes = TileGeo<N>::bytes;
-    cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+static cudaError_t configure_one() {
+    cudaError_t e = cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TileGeo<N>::bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_march<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, MarchGeo<N>::bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_march<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    return e;
 }
 
 template <int N>
-static void configure_modes() {
-    configure_one<N, kFwd>();
-    configure_one<N, kRcv>();
-    configure_one<N, kRec>();
+static cudaError_t configure_modes() {
+    cudaError_t e = configure_one<N, kFwd>();
+    if (e == cudaSuccess) e = configure_one<N, kRcv>();
+    if (e == cudaSuccess) e = configure_one<N, kRec>();
+    return e;
 }
 
 // Shared-memory attributes of the step kernels of half-order N on the current
 // device (a per-device setting): ouc_create sets them for its device, the
 // no-allocation entry point at its set-up on each device.
-void configure_step_kernels(int N) {
-    if (N == 2) configure_modes<2>();
-    if (N == 5) configure_modes<5>();
-    if (N == 6) configure_modes<6>();
+cudaError_t configure_step_kernels(int N) {
+    if (N == 2) return configure_modes<2>();
+    if (N == 5) return configure_modes<5>();
+    if (N == 6) return configure_modes<6>();
+    return cudaErrorInvalidValue;
+}
+
+int march_segments(Mode mode, const StepArgs& a) {
+    constexpr int RB = 16;
+    const int row0 = mode == kRec ? (a.L / RB) * RB : 0;
+    const int row_end = mode == kRec ? a.X - a.L : (a.X + RB - 1) / RB * RB;
+    return (row_end - row0 + a.seg_rows - 1) / a.seg_rows;
 }
 
 template <int N, int MODE>
 static void launch_one(const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
+    if (a.seg_rows > 0) {
+        const int nseg = march_segments((Mode)MODE, a);
+        k_march<N, MODE><<<dim3(nseg * a.tiles_z, nshots), kThreads, MarchGeo<N>::bytes, s>>>(a);
+        return;
+    }
     constexpr int bytes = TileGeo<N>::bytes;
     k_step<N, MODE><<<dim3(tiles_x * a.tiles_z, nshots), kThreads, bytes, s>>>(a);
 }
@@ -140,7 +162,7 @@ __global__ void k_finalize(const FinalizeArgs f) {
             sps += (double)lps;
             sil += f.illum_scale * (f.comp[2] ? (double)f.acc[2][g] - (double)f.comp[2][g] : (double)f.acc[2][g]);
         }
-        if (f.stack[0]) {
+        if (f.stack[0] && !(f.status && *f.status)) {   // a failed batch leaves the stack as it was
             f.stack[0][o] += spp;
             f.stack[1][o] += sps;
             f.stack[2][o] += sil;
@@ -310,6 +332,26 @@ void launch_mute(float* gx, float* gz, int X, int nt, int sx, int sz, int rz, in
                  cudaStream_t s) {
     dim3 grid((X + 127) / 128, nt < 1024 ? nt : 1024);
     k_mute<<<grid, 128, 0, s>>>(gx, gz, X, nt, sx, sz, rz, t0, dt, dh, v);
+}
+
+// Non-finite detector: bit 1 of *status when any of the n floats at p is
+// NaN or infinite (an unstable or overflowing run).  One vote per warp, one
+// atomic per warp that saw one; the data is only read.
+__global__ void k_finite(const float* __restrict__ p, size_t n, int* status) {
+    bool bad = false;
+    const size_t n4 = n / 4;
+    const float4* p4 = reinterpret_cast<const float4*>(p);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 v = p4[i];
+        bad |= !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w);
+    }
+    for (size_t i = 4 * n4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        bad |= !isfinite(p[i]);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, 2);
+}
+
+void launch_finite_check(const float* p, size_t n, int* status, cudaStream_t s) {
+    k_finite<<<1184, 256, 0, s>>>(p, n, status);   // 8 CTAs of 256 per SM, grid-stride
 }
 
 // out[c][r] = in[r][c] through a 32x33 shared tile.

@@ -120,8 +120,11 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
         float* ptr = nullptr;
         if (cudaGetSymbolAddress((void**)&ptr, g_scratch) != cudaSuccess || !ptr) return OUC_ECUDA;
         // the step kernels' shared-memory opt-in is a per-device setting too
-        for (int n : {2, 5, 6}) configure_step_kernels(n);
-        if (cudaGetLastError() != cudaSuccess) return OUC_ECUDA;
+        for (int n : {2, 5, 6})
+            if (configure_step_kernels(n) != cudaSuccess) {
+                cudaGetLastError();   // this call's own failure: clear it, report it
+                return OUC_ECUDA;
+            }
         g_scratch_addr[dev] = ptr;
     }
     float* base = g_scratch_addr[dev];

@@ -12,6 +12,8 @@
 // Field pointers passed to kernels point at cell (0, 0): element (i, j) is
 // f[i * pitch + j] for i in [-GX, Xc+GX) and j in [-ZOFF, Zc+ZOFF).
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
 
@@ -125,6 +127,8 @@ struct StepArgs {
     int strip_prec;                   // StripPrec of the strips
     int comp_image;                   // kRec: compensated (Kahan) imaging sums, comp[] below
     int density;                      // variable density: scale the U-stage by the buoyancy
+    int seg_rows;                     // > 0: the x-marching kernel, segments of this many rows (a multiple of 16)
+    int* err;                         // device word: kernels record OUC_ETIMEOUT-class failures here (or null)
     float a[6];                       // stencil weights a_1..a_N
     float dx, dz, dt, dt2;
     float rdx, rdz;                   // RN(1/dx), RN(1/dz)
@@ -164,6 +168,7 @@ struct FinalizeArgs {
     float* img;            // [shot][2][nx][nz] dense, or null
     double* stack[3];      // nx*nz dense FP64: PP, PS, illumination (or null)
     double illum_scale;    // illumination into the stack x this (imaged levels: every K-th)
+    const int* status;     // device status word (or null): nonzero leaves the stack untouched
 };
 
 // Source-wavefield snapshots (ouc_config.snapshot_every = K >= 1): the
@@ -214,13 +219,17 @@ struct GradStackArgs {
 
 // Host-side launchers (kernels.cu)
 int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s);
-void configure_step_kernels(int N);
+// Segments of the x-marching kernel for a launch (rows of the widest shot).
+int march_segments(Mode mode, const StepArgs& a);
+cudaError_t configure_step_kernels(int N);
 int step_smem_bytes(int N);
 void launch_image_only(const StepArgs& a, int nshots, cudaStream_t s);
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s);
 void launch_mute(float* gx, float* gz, int X, int nt, int sx, int sz, int rz, int t0, float dt, float dh, float v,
                  cudaStream_t s);
 void launch_transpose(const float* in, float* out, int rows, int cols, cudaStream_t s);
+// Bit 1 of *status when any of n floats (16-byte aligned) is not finite.
+void launch_finite_check(const float* p, size_t n, int* status, cudaStream_t s);
 void launch_pack_fields(const float* const* f, int nf, int X, int Z, int pitch, float* out, cudaStream_t s);
 void launch_strip_pack(const ShotDesc* shots, int nshots, int slot, int ring, size_t strip_slot, cudaStream_t s);
 void launch_snap_store(const SnapArgs& a, int nshots, cudaStream_t s);

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import ouc_b200 as o
+from helpers import golden_shot, load_golden, make_context
 from ouc_b200 import models
 
 pytestmark = pytest.mark.gpu
@@ -77,3 +78,22 @@ def test_subgrid_arguments_are_checked(model_and_wavelet):
             ctx.survey_forward(shots[:1], [(200, 300)], w)      # source outside its aperture
         with pytest.raises(o.OucError):
             ctx.survey_forward(shots[:1], [(0, 400)], w)        # beyond the model
+
+
+def test_migrate_on_one_rank_equals_rtm_batch_and_stack():
+    """survey.migrate at world size 1 (the function a multi-GPU survey calls
+    on every rank) gives the stack of rtm_batch over the same shots."""
+    from ouc_b200 import survey
+    g = load_golden("g72x56n5")
+    shots = [golden_shot(g)]
+    for sx in (9, 30, 41):
+        s = golden_shot(g)
+        s.sx = sx
+        shots.append(s)
+    with make_context(g, max_batch=2) as a:
+        a.rtm_batch(shots, g["src"])
+        ref = a.stack(reset=True)
+    with make_context(g, max_batch=2) as b:
+        got = survey.migrate(b, shots, g["src"])
+    for x, y in zip(got, ref):
+        assert np.array_equal(x, y)
