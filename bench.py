@@ -385,13 +385,41 @@ def main():
         e2e_s = float(tt.item())
     e2e = cells * e2e_steps * world / e2e_s / 1e9
 
-    # roofline of the dominant kernel: the fused forward step (k_step, forward mode)
+    # rooflines of the three step kernels.  Algorithmic bytes per launch
+    # (each byte moved once, the batch's B shots): forward and receiver 56 B
+    # per padded cell + 48 B per damped cell per axis (+ the strip write of
+    # the ring, resp. the record row read); reconstruction + imaging 56 B +
+    # 24 B (three accumulators read and written) per interior cell + the
+    # strip read.  The forward launch is timed over the timed region (its
+    # phase holds nothing else); all three are also timed one launch kind at
+    # a time on the state the last batch left (ouc_time_step_kernels).
     peak, peak_kind = measured_peak()
-    per_launch_ms = statistics.median(fwd_ms) / nt
-    abytes = algorithmic_bytes_forward(cfg, X, ring_cells(cfg), 4 if args.strips == "fp32" else 2) * B
-    achieved = abytes / (per_launch_ms / 1e3) / 1e9
+    sb = 4 if args.strips == "fp32" else 2
+    C, Ci, L = X * cfg.Z, cfg.nx * cfg.nz, cfg.npml
+    damp = 48 * ((2 * L - 1) * cfg.Z + (2 * L - 1) * X)
+    alg = {"forward": (56 * C + damp + 8 * ring_cells(cfg) * sb) * B,
+           "receiver": (56 * C + damp + 8 * X) * B,
+           "reconstruction": (80 * Ci + 8 * ring_cells(cfg) * sb) * B}
+    seg = mig.step_kernel()
+    kname = (lambda m: f"k_march<{cfg.half_order}, {m}> ({seg}-row segments, 16-row blocks)" if seg else
+             f"k_step<{cfg.half_order}, {m}> (32 x 64 tiles)")
+    kern = {}
+    if not args.snapshot_every:
+        iso = mig.time_step_kernels(B, reps=20)
+        for k, name in enumerate(("forward", "receiver", "reconstruction")):
+            a_gbs = alg[name] / (iso[k] / 1e3) / 1e9
+            kern[name] = {"kernel": kname(name), "launch_ms": iso[k], "algorithmic_bytes_per_launch": alg[name],
+                          "achieved": a_gbs, "frac": a_gbs / peak}
+    per_launch_ms = statistics.median(fwd_ms) / nt        # forward launch, over the timed region
+    dom = max(kern, key=lambda k: kern[k]["launch_ms"]) if kern else "forward"
+    if dom == "forward":
+        r_ms, r_bytes, r_src = per_launch_ms, alg["forward"], "forward phase of the timed region / nt"
+    else:
+        r_ms, r_bytes, r_src = kern[dom]["launch_ms"], alg[dom], "isolated launches (ouc_time_step_kernels)"
+    achieved = r_bytes / (r_ms / 1e3) / 1e9
     tr = committed_traffic()
-    traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name and tr.get("batch") == B else None
+    traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name and tr.get("batch") == B and \
+        tr.get("kernel") == kname(dom) else None
 
     # saved source wavefield per shot: 8 ring fields per step (strip form) or
     # the two P components of every K-th imaging level (snapshot form)
@@ -424,11 +452,14 @@ def main():
                     "h2d_bytes_per_step": B * 2 * nt * X * 4 + nt * 4,
                     "d2h_bytes_per_step": B * 2 * cfg.nx * cfg.nz * 4 + 3 * cfg.nx * cfg.nz * 8,
                     "shots_per_hour": 3600.0 * B * e2e_steps * world / e2e_s},
-            "roofline": {"kernel": f"k_step<5, forward> (fused S+U stage, CPML, strip save), {B} shots per launch",
+            "roofline": {"kernel": f"{kname(dom)}, {B} shots per launch (the slowest of the three step kernels)",
                          "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": abytes,
-                         "launch_ms": per_launch_ms, "traffic": traffic},
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": r_bytes,
+                         "launch_ms": r_ms, "launch_ms_from": r_src, "traffic": traffic,
+                         "forward_launch_ms_timed_region": per_launch_ms,
+                         "backward_step_ms_timed_region": statistics.median(bwd_ms) / nt},
+            "step_kernels": kern,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clk,

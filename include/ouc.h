@@ -295,10 +295,16 @@ int ouc_survey_rtm(ouc_ctx* ctx, int nshots, const ouc_shot* shots, const ouc_ap
  * faster to win); *best_batch and *ns_per_cell may be NULL.  Later
  * ouc_rtm_batch / ouc_survey_* calls advance that many shots per launch.
  * ouc_set_run_batch sets it directly (1 .. cfg.max_batch), e.g. from a cache
- * of earlier tuning results.  The tile shape (32 x 64 cells per CTA) is fixed
- * at compile time. */
+ * of earlier tuning results.  It keeps the current step-kernel geometry;
+ * ouc_tune below chooses both. */
 int ouc_tune_batch(ouc_ctx* ctx, int steps, int* best_batch, float* ns_per_cell);
 int ouc_set_run_batch(ouc_ctx* ctx, int n);
+/* Joint tuning of the launch batch and the step-kernel geometry: for each
+ * batch candidate, forward steps are timed with the tile kernel and with the
+ * x-marching kernel at segment lengths 64 .. 512 rows; the fastest geometry
+ * per batch is kept and the batch is chosen as ouc_tune_batch does.  Both
+ * choices are applied to the context; each output pointer may be NULL. */
+int ouc_tune(ouc_ctx* ctx, int steps, int* best_batch, int* best_seg_rows, float* ns_per_cell);
 
 /* Step-kernel geometry.  seg_rows > 0 (a multiple of 16): the x-marching
  * kernel, each CTA walking a 64-column strip down a segment of that many rows
@@ -310,6 +316,13 @@ int ouc_set_run_batch(ouc_ctx* ctx, int n);
  * loops (they are captured again on next use). */
 int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows);
 int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows);
+
+/* Device time of one launch of each step kernel at batch n (ms[0] forward,
+ * ms[1] receiver, ms[2] reconstruction + imaging), averaged over `reps`
+ * launches after one warm-up, on the state the last RTM batch of n shots
+ * left (call it right after such a batch; the state is consumed).  CUDA
+ * events on the context stream. */
+int ouc_time_step_kernels(ouc_ctx* ctx, int n, int reps, float* ms);
 
 /* Forward modeling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they need

@@ -53,7 +53,9 @@ SIGNATURES = {
     "ouc_destroy": (C.c_int, [_vp]),
     "ouc_dims": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "ouc_set_step_kernel": (C.c_int, [_vp, C.c_int]),
+    "ouc_tune": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "ouc_get_step_kernel": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "ouc_time_step_kernels": (C.c_int, [_vp, C.c_int, C.c_int, _fp]),
     "ouc_stream": (_vp, [_vp]),
     "ouc_last_timing": (C.c_int, [_vp, C.POINTER(ouc_timing)]),
     "ouc_device_bytes": (C.c_size_t, [_vp]),

@@ -371,6 +371,13 @@ class Context:
         multiple of 16), or 0 for the 32 x 64 tile kernel (ouc_set_step_kernel)."""
         check(lib().ouc_set_step_kernel(self._h, int(seg_rows)), self._h)
 
+    def time_step_kernels(self, n, reps=10):
+        """Device ms per launch of the forward, receiver and reconstruction
+        step kernels at batch n, on the state of the last RTM batch."""
+        ms = np.zeros(3, np.float32)
+        check(lib().ouc_time_step_kernels(self._h, int(n), int(reps), _p(ms)), self._h)
+        return [float(x) for x in ms]
+
     def step_kernel(self):
         v = C.c_int()
         check(lib().ouc_get_step_kernel(self._h, C.byref(v)), self._h)

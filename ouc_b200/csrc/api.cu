@@ -837,6 +837,34 @@ int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows) {
     return OUC_OK;
 }
 
+int ouc_time_step_kernels(ouc_ctx* ctx, int n, int reps, float* ms) {
+    if (!ctx || !ms || n < 1 || n > ctx->batch || reps < 1) return OUC_EINVAL;
+    if (!ctx->strips || ctx->nt < 4) return fail(ctx, OUC_ESTATE, "run an RTM batch of these shots first");
+    cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;
+    int rc;
+    const int t = ctx->nt / 2;
+    Side s = ctx->src, r = ctx->rcv;
+    StepArgs a = base_args(ctx);
+    a.record = 0;
+    a.save = ctx->cfg.snapshot_every == 0;
+    StepArgs ar = rcv_args(ctx), as = rec_args(ctx);
+    const bool exact = ctx->cfg.strip_level == OUC_STRIP_EXACT;
+    for (int kind = 0; kind < 3; ++kind) {
+        for (int k = 0; k < reps + 1; ++k) {   // one warm-up launch, then `reps` timed
+            if (k == 1) CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+            if (kind == 0) rc = fwd_step(ctx, a, s, n, t);
+            else if (kind == 1) rc = rcv_step(ctx, ar, r, n, t);
+            else rc = rec_step(ctx, as, s, r, n, t, exact, true);
+            if (rc) return rc;
+        }
+        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        ms[kind] = elapsed(ctx->ev[0], ctx->ev[1]) / reps;
+    }
+    return check_status(ctx);
+}
+
 int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows) {
     if (!ctx || !seg_rows) return OUC_EINVAL;
     *seg_rows = ctx->seg_rows;

@@ -308,6 +308,45 @@ int ouc_tune_batch(ouc_ctx* ctx, int steps, int* best_batch, float* ns_per_cell)
     return OUC_OK;
 }
 
+int ouc_tune(ouc_ctx* ctx, int steps, int* best_batch, int* best_seg_rows, float* ns_per_cell) {
+    if (!ctx || steps < 1) return OUC_EINVAL;
+    cudaSetDevice(ctx->device);
+    ctx->step_phase = ouc_ctx::kIdle;
+    if (cudaMemsetAsync(ctx->d_wavelet, 0, (size_t)ctx->nt * 4, ctx->stream) != cudaSuccess) return OUC_ECUDA;
+    std::vector<int> batches, segs = {0};
+    for (int n = 1; n < ctx->batch; n *= 2) batches.push_back(n);
+    batches.push_back(ctx->batch);
+    for (int r : {64, 96, 128, 192, 256, 384, 512})
+        if (r < ctx->X + 16) segs.push_back(r);
+    int best = 1, best_seg = ctx->seg_rows;
+    float best_ns = 0.f;
+    for (int n : batches) {
+        int seg_n = 0;
+        float ns_n = 0.f;
+        for (int r : segs) {
+            int rc = ouc_set_step_kernel(ctx, r);
+            float ms = 0.f;
+            if (!rc) rc = ouc::survey::time_batch(ctx, n, steps, &ms);
+            if (rc) return rc;
+            const float ns = ms * 1e6f / ((float)n * steps * ctx->X * ctx->Z);
+            if (ns_n == 0.f || ns < ns_n) { ns_n = ns; seg_n = r; }
+        }
+        // a larger batch must be clearly faster to be preferred (memory per shot)
+        if (best_ns == 0.f || ns_n < 0.97f * best_ns) {
+            best = n;
+            best_ns = ns_n;
+            best_seg = seg_n;
+        }
+    }
+    ctx->run_batch = best;
+    const int rc = ouc_set_step_kernel(ctx, best_seg);
+    if (rc) return rc;
+    if (best_batch) *best_batch = best;
+    if (best_seg_rows) *best_seg_rows = best_seg;
+    if (ns_per_cell) *ns_per_cell = best_ns;
+    return OUC_OK;
+}
+
 int ouc_set_run_batch(ouc_ctx* ctx, int n) {
     if (!ctx || n < 1 || n > ctx->batch) return OUC_EINVAL;
     ctx->run_batch = n;

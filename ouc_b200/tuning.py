@@ -1,11 +1,13 @@
-"""Autotuned launch batch, persisted across runs.
+"""Autotuned launch batch and step-kernel geometry, persisted across runs.
 
-``tune(ctx)`` returns the number of shots per launch for this context's
-grid: from the JSON cache when an entry for (padded grid, stencil half-order,
-GPU name, library version) exists, otherwise measured by ``ouc_tune_batch``
-(a few timed forward steps at 1, 2, 4, ... up to cfg.max_batch shots per
-launch) and stored.  The cache file is ``$OUC_TUNE_CACHE`` or
-``~/.cache/ouc_b200/tune.json``.
+``tune(ctx)`` returns the number of shots per launch for this context's grid
+and applies it together with the step-kernel geometry (32 x 64 tiles, or the
+x-marching kernel with its segment length): from the JSON cache when an
+entry for (padded grid, stencil half-order, max batch, GPU name, library
+version) exists, otherwise measured by ``ouc_tune`` (timed forward steps at
+1, 2, 4, ... up to cfg.max_batch shots per launch, each with the tile kernel
+and with segments of 64 .. 512 rows) and stored.  The cache file is
+``$OUC_TUNE_CACHE`` or ``~/.cache/ouc_b200/tune.json``.
 """
 from __future__ import annotations
 
@@ -34,21 +36,25 @@ def _load(path):
 
 
 def tune(ctx, steps=20, path=None, device_name=None, force=False):
-    """Shots per launch for `ctx` (applied to it); returns (batch, ns per
-    cell-update or None when taken from the cache, from_cache)."""
+    """Shots per launch for `ctx` (applied to it, with the tuned step-kernel
+    geometry); returns (batch, ns per cell-update or None when taken from the
+    cache, from_cache).  ``ctx.step_kernel()`` reads the geometry chosen."""
     path = path or cache_path()
     if device_name is None:
         import torch
         device_name = torch.cuda.get_device_name(ctx.cfg.device).replace(" ", "_")
     key = _key(ctx, device_name)
     cache = _load(path)
-    if not force and key in cache and 1 <= int(cache[key]["batch"]) <= max(1, ctx.cfg.max_batch):
-        check(lib().ouc_set_run_batch(ctx.handle, int(cache[key]["batch"])), ctx.handle)
-        return int(cache[key]["batch"]), None, True
+    ent = cache.get(key)
+    if not force and ent and 1 <= int(ent.get("batch", 0)) <= max(1, ctx.cfg.max_batch) and "seg_rows" in ent:
+        check(lib().ouc_set_run_batch(ctx.handle, int(ent["batch"])), ctx.handle)
+        check(lib().ouc_set_step_kernel(ctx.handle, int(ent["seg_rows"])), ctx.handle)
+        return int(ent["batch"]), None, True
     best = C.c_int()
+    seg = C.c_int()
     ns = C.c_float()
-    check(lib().ouc_tune_batch(ctx.handle, int(steps), C.byref(best), C.byref(ns)), ctx.handle)
-    cache[key] = {"batch": best.value, "ns_per_cell_update": ns.value, "steps": steps}
+    check(lib().ouc_tune(ctx.handle, int(steps), C.byref(best), C.byref(seg), C.byref(ns)), ctx.handle)
+    cache[key] = {"batch": best.value, "seg_rows": seg.value, "ns_per_cell_update": ns.value, "steps": steps}
     os.makedirs(os.path.dirname(path), exist_ok=True)
     tmp = path + ".tmp"
     with open(tmp, "w") as f:

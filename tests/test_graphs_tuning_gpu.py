@@ -58,7 +58,10 @@ def test_autotuner_picks_a_candidate_and_caches_it(tmp_path):
             check(lib().ouc_set_run_batch(ctx.handle, 9), ctx.handle)
         w, t0 = o.ricker(25.0, 5e-4, NT)
         imgs = ctx.rtm_batch([o.Shot(sx=40, sz=2, rz=2, t0=t0)] * 3, w)   # runs with the tuned batch
+        seg = ctx.step_kernel()
     assert b1 in (1, 2, 4, 8) and not cached1 and ns > 0
     assert b2 == b1 and cached2
-    assert list(json.load(open(path)).values())[0]["batch"] == b1
+    ent = list(json.load(open(path)).values())[0]
+    assert ent["batch"] == b1 and ent["seg_rows"] == seg
+    assert seg == 0 or (seg % 16 == 0 and 64 <= seg <= 512)
     assert np.array_equal(imgs[0][0], imgs[2][0], equal_nan=True)
