@@ -44,6 +44,9 @@ using bf16 = __nv_bfloat16;
 constexpr int kTile = 128;            // GEMM M: pixels per tile
 constexpr int kPC = kTile + 4;        // patch columns (2 + 2 halo)
 constexpr int kTaps = 25;
+constexpr int kMaxPairs = 32 * 32;     // (cin, cout) pairs of the widest layer
+constexpr int kMaxRowBlocks = 64;      // row blocks of k_wgrad
+constexpr int kBgradBlocks = 256;      // blocks of k_bgrad (8 warps each)
 constexpr int kThreadsConv = 128;
 
 struct LayerDims {
@@ -316,7 +319,7 @@ cudaError_t launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
 // grid.y = row blocks; each thread owns up to 4 (ci, co) pairs.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(256) k_wgrad(int n, int H, int W, const bf16* x, const bf16* g, int cin_real,
-                                               int cout_real, float* dw) {
+                                               int cout_real, float* part) {
     constexpr int PX = 32;
     __shared__ float xs[PX][CIN + 1];
     __shared__ float gs[PX][COUT + 1];
@@ -353,30 +356,51 @@ __global__ void __launch_bounds__(256) k_wgrad(int n, int H, int W, const bf16* 
             }
         }
     }
+    // this row block's partial sums, reduced in a fixed order by k_wgrad_sum
+    // (no atomics: training is reproducible run to run)
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int pr = threadIdx.x + 256 * k;
-        if (pr < npairs) {
-            const int ci = pr % cin_real, co = pr / cin_real;
-            atomicAdd(dw + ((size_t)co * cin_real + ci) * kTaps + tap, acc[k]);
-        }
+        if (pr < npairs) part[((size_t)blockIdx.y * kTaps + tap) * kMaxPairs + pr] = acc[k];
+    }
+}
+
+// dw[co][ci][tap] += sum over the row blocks, in block order.
+__global__ void k_wgrad_sum(int nblocks, int cin_real, int cout_real, const float* part, float* dw) {
+    const int npairs = cin_real * cout_real;
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < kTaps * npairs; i += blockDim.x * gridDim.x) {
+        const int tap = i / npairs, pr = i - tap * npairs;
+        float s = 0.f;
+        for (int b = 0; b < nblocks; ++b) s += part[((size_t)b * kTaps + tap) * kMaxPairs + pr];
+        const int ci = pr % cin_real, co = pr / cin_real;
+        dw[((size_t)co * cin_real + ci) * kTaps + tap] += s;
     }
 }
 
 template <int COUT>
-__global__ void k_bgrad(size_t npix, const bf16* g, int cout_real, float* db) {
+__global__ void k_bgrad(size_t npix, const bf16* g, int cout_real, float* part) {
     float acc[COUT];
 #pragma unroll
     for (int c = 0; c < COUT; ++c) acc[c] = 0.f;
     for (size_t p = threadIdx.x + (size_t)blockIdx.x * blockDim.x; p < npix; p += (size_t)blockDim.x * gridDim.x)
 #pragma unroll
         for (int c = 0; c < COUT; ++c) acc[c] += __bfloat162float(g[p * COUT + c]);
+    const int wid = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     for (int c = 0; c < cout_real; ++c) {
         float v = acc[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(db + c, v);
+        if ((threadIdx.x & 31) == 0) part[(size_t)wid * 32 + c] = v;   // one slot per warp and channel
     }
+}
+
+// db[c] += sum over the warps' partial sums, in warp order.
+__global__ void k_bgrad_sum(int nwarps, int cout_real, const float* part, float* db) {
+    const int c = threadIdx.x;
+    if (c >= cout_real) return;
+    float s = 0.f;
+    for (int w = 0; w < nwarps; ++w) s += part[(size_t)w * 32 + c];
+    db[c] += s;
 }
 
 // float [P][creal] -> bf16 [P][cpad], zero-padded channels
@@ -456,6 +480,7 @@ struct ouc_cnn {
     bf16* wf[4] = {};            // packed forward weights
     bf16* wd[4] = {};            // packed input-gradient weights (layers 1..3)
     int* err = nullptr;
+    float* part = nullptr;       // gradient partial sums, reduced in a fixed order (kMaxRowBlocks x 25 x kMaxPairs)
     // activations of the last forward
     int n = 0, H = 0, W = 0;
     size_t cap = 0;              // pixels the buffers hold
@@ -519,7 +544,8 @@ int ouc_cnn_create(int device, ouc_cnn** out) {
     const size_t pb = (size_t)kNParams * 4;
     bool ok = cudaMalloc(&net->params, pb) == cudaSuccess && cudaMalloc(&net->grads, pb) == cudaSuccess &&
               cudaMalloc(&net->adam_m, pb) == cudaSuccess && cudaMalloc(&net->adam_v, pb) == cudaSuccess &&
-              cudaMalloc(&net->err, sizeof(int)) == cudaSuccess;
+              cudaMalloc(&net->err, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&net->part, (size_t)kMaxRowBlocks * kTaps * kMaxPairs * sizeof(float)) == cudaSuccess;
     for (int l = 0; l < 4 && ok; ++l) {
         ok = cudaMalloc(&net->wf[l], (size_t)kTaps * kL[l].cin_pad * kL[l].cout_pad * 2) == cudaSuccess;
         if (ok && l > 0) ok = cudaMalloc(&net->wd[l], (size_t)kTaps * kL[l].cin_pad * kL[l].cout_pad * 2) == cudaSuccess;
@@ -546,7 +572,7 @@ int ouc_cnn_destroy(ouc_cnn* net) {
     if (!net) return OUC_OK;
     cudaSetDevice(net->device);
     cudaDeviceSynchronize();
-    cudaFree(net->params); cudaFree(net->grads); cudaFree(net->adam_m); cudaFree(net->adam_v); cudaFree(net->err);
+    cudaFree(net->params); cudaFree(net->grads); cudaFree(net->adam_m); cudaFree(net->adam_v); cudaFree(net->err); cudaFree(net->part);
     for (auto* p : net->wf) cudaFree(p);
     for (auto* p : net->wd) cudaFree(p);
     cudaFree(net->x0); cudaFree(net->g16);
@@ -601,12 +627,14 @@ int ouc_cnn_backward_dev(ouc_cnn* net, const float* d_gout, void* stream) {
     const int n = net->n, H = net->H, W = net->W;
     const size_t P = (size_t)n * H * W;
     const int rows = n * H;
-    const dim3 wg(kTaps, rows < 64 ? rows : 64);
+    const dim3 wg(kTaps, rows < kMaxRowBlocks ? rows : kMaxRowBlocks);
     k_to_bf16<<<1024, 256, 0, s>>>(P, OUC_CNN_OUT, 16, d_gout, net->g16);
     // layer 4: weights and bias, then the gradient into layer 3's output
     float* gp = net->grads;
-    k_wgrad<32, 16><<<wg, 256, 0, s>>>(n, H, W, net->y[2], net->g16, kL[3].cin, kL[3].cout, gp + p_offset(3));
-    k_bgrad<16><<<256, 256, 0, s>>>(P, net->g16, kL[3].cout, gp + p_offset(3) + w_count(3));
+    k_wgrad<32, 16><<<wg, 256, 0, s>>>(n, H, W, net->y[2], net->g16, kL[3].cin, kL[3].cout, net->part);
+    k_wgrad_sum<<<64, 256, 0, s>>>(wg.y, kL[3].cin, kL[3].cout, net->part, gp + p_offset(3));
+    k_bgrad<16><<<kBgradBlocks, 256, 0, s>>>(P, net->g16, kL[3].cout, net->part);
+    k_bgrad_sum<<<1, 32, 0, s>>>(kBgradBlocks * 8, kL[3].cout, net->part, gp + p_offset(3) + w_count(3));
     ConvArgs a{};
     a.n = n; a.H = H; a.W = W; a.err = net->err;
     a.x = net->g16; a.w = net->wd[3]; a.mask = net->y[2]; a.y = net->g[0];
@@ -614,15 +642,19 @@ int ouc_cnn_backward_dev(ouc_cnn* net, const float* d_gout, void* stream) {
     // layers 3 and 2
     for (int l = 2; l >= 1; --l) {
         const bf16* gl = net->g[(2 - l) & 1];
-        k_wgrad<32, 32><<<wg, 256, 0, s>>>(n, H, W, net->y[l - 1], gl, kL[l].cin, kL[l].cout, gp + p_offset(l));
-        k_bgrad<32><<<256, 256, 0, s>>>(P, gl, kL[l].cout, gp + p_offset(l) + w_count(l));
+        k_wgrad<32, 32><<<wg, 256, 0, s>>>(n, H, W, net->y[l - 1], gl, kL[l].cin, kL[l].cout, net->part);
+        k_wgrad_sum<<<64, 256, 0, s>>>(wg.y, kL[l].cin, kL[l].cout, net->part, gp + p_offset(l));
+        k_bgrad<32><<<kBgradBlocks, 256, 0, s>>>(P, gl, kL[l].cout, net->part);
+        k_bgrad_sum<<<1, 32, 0, s>>>(kBgradBlocks * 8, kL[l].cout, net->part, gp + p_offset(l) + w_count(l));
         a.x = gl; a.w = net->wd[l]; a.mask = net->y[l - 1]; a.y = net->g[(3 - l) & 1];
         if (launch_conv<32, 32, kDgrad>(a, net->sms, s) != cudaSuccess) return OUC_ECUDA;
     }
     // layer 1
     const bf16* g1 = net->g[0];
-    k_wgrad<16, 32><<<wg, 256, 0, s>>>(n, H, W, net->x0, g1, kL[0].cin, kL[0].cout, gp + p_offset(0));
-    k_bgrad<32><<<256, 256, 0, s>>>(P, g1, kL[0].cout, gp + p_offset(0) + w_count(0));
+    k_wgrad<16, 32><<<wg, 256, 0, s>>>(n, H, W, net->x0, g1, kL[0].cin, kL[0].cout, net->part);
+    k_wgrad_sum<<<64, 256, 0, s>>>(wg.y, kL[0].cin, kL[0].cout, net->part, gp + p_offset(0));
+    k_bgrad<32><<<kBgradBlocks, 256, 0, s>>>(P, g1, kL[0].cout, net->part);
+    k_bgrad_sum<<<1, 32, 0, s>>>(kBgradBlocks * 8, kL[0].cout, net->part, gp + p_offset(0) + w_count(0));
     return cudaGetLastError() == cudaSuccess ? OUC_OK : OUC_ECUDA;
 }
 

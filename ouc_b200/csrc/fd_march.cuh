@@ -21,8 +21,11 @@
 // the only S-stage work done twice).  Between blocks the producer lanes of
 // warp 0 issue the next block's row copies as soon as the stage is free.
 //
-// Waits on the copies are bounded: after ~1 s of polling the CTA records
-// OUC_ETIMEOUT in *StepArgs::err and carries on (the host reports it).
+// Waits on the copies are bounded: after ~20 ms of polling the CTA records
+// the failure, issues no further copies, gives the copies in flight one more
+// bounded wait before it exits and sets bit 0 of *StepArgs::err; every later
+// CTA and launch that sees the bit returns at once, and the host reports
+// OUC_ETIMEOUT after the call.
 #pragma once
 #include <cstdint>
 
@@ -84,11 +87,12 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait on phase `parity`: false after about one second of polling.
+// Bounded wait on phase `parity`: false after about 20 ms of polling (a row
+// copy takes microseconds).
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
-    for (int k = 0; k < (1 << 24); ++k) {
+    for (int k = 0; k < (1 << 17); ++k) {
         if (mbar_test(b, parity)) return true;
-        if (k >= 32) __nanosleep(64);
+        if (k >= 32) __nanosleep(128);
     }
     return false;
 }
@@ -167,6 +171,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
     const int row_end = MODE == kRec ? X - L : (X + RB - 1) / RB * RB;
     const int xs = row0 + seg * p.seg_rows;
     if (xs >= row_end) return;   // beyond this shot's rows
+    if (p.err && (*(volatile int*)p.err & 1)) return;   // an earlier copy wait gave up: do nothing more
     const int xe = min(xs + p.seg_rows, row_end);
     const int z0 = (p.tile_z0 + strip) * TZ;
     const int nblk = (xe - xs + RB - 1) / RB;
@@ -193,6 +198,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
         issue_model<N>(p, gm, xs - RB + SHX, z0, sMod, &bars[1], lane);
     }
     bool timed_out = false;
+    int nraw = 1, nmod = 1;   // stage phases issued so far (the prologue issued one of each)
 
     // per-strip flags (uniform over the item)
     const bool pz = z0 - HS < L || z0 + TZ + HS - 1 >= Z - L;        // S region meets the z damping
@@ -205,7 +211,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
         const int ubase = o + SHX + N;   // first new U row
         const int sbase = o + SHX;       // first new S row
         // ---- 1. U = P + S for the new U rows ----------------------------------------
-        if (!mbar_wait(&bars[0], (unsigned)(k + 2) & 1u)) timed_out = true;
+        if (!timed_out && !mbar_wait(&bars[0], (unsigned)(k + 2) & 1u)) timed_out = true;
         for (int idx = tid; idx < RB * G::UCOLS; idx += kThreads) {
             const int r = idx / G::UCOLS, c4 = idx - r * G::UCOLS;
             const float* s = sRaw + r * UC + 4 * c4;
@@ -236,15 +242,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
                 sUz[oo] = strip_get(p, su, am, kSUz, kSUz * R + ri);
             });
         }
-        __syncthreads();
-        if (warp == 0 && k + 1 < nblk) {
-            fence_proxy_async();
-            issue_raw<N>(p, off, ubase + RB, z0, sRaw, &bars[0], lane);
+        timed_out = __syncthreads_or(timed_out);   // uniform over the CTA from here on
+        if (k + 1 < nblk && !timed_out) {
+            ++nraw;
+            if (warp == 0) {
+                fence_proxy_async();
+                issue_raw<N>(p, off, ubase + RB, z0, sRaw, &bars[0], lane);
+            }
         }
 
         // ---- 2. S-stage on the new S rows ---------------------------------------------
         if (k >= -1) {
-            if (!mbar_wait(&bars[1], (unsigned)(k + 1) & 1u)) timed_out = true;
+            if (!timed_out && !mbar_wait(&bars[1], (unsigned)(k + 1) & 1u)) timed_out = true;
             const bool px = sbase < L || sbase + RB - 1 >= X - L;
             const bool border = MODE != kRec && !(sbase >= N && sbase + RB <= X - N && z0 - HS >= N && z0 + TZ + HS <= Z - N);
             if (tid < G::sItems) {
@@ -365,10 +374,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
                 if (p.strip_prec == kStripF16) amax_commit<6>(d.amax + (size_t)p.t * kStripFields, kSTh, m);
             }
         }
-        __syncthreads();
-        if (warp == 0 && k >= -1 && k + 1 < nblk) {
-            fence_proxy_async();
-            issue_model<N>(p, gm, sbase + RB, z0, sMod, &bars[1], lane);
+        timed_out = __syncthreads_or(timed_out);
+        if (k >= -1 && k + 1 < nblk && !timed_out) {
+            ++nmod;
+            if (warp == 0) {
+                fence_proxy_async();
+                issue_model<N>(p, gm, sbase + RB, z0, sMod, &bars[1], lane);
+            }
         }
         // ---- shift of the U rows: [RB, UR) -> [0, UR - RB) ---------------------------
         {
@@ -614,8 +626,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
             }
         }
     }
-    if (timed_out && p.err) atomicOr(p.err, 1);
-    // no copy is left in flight: every issued stage was waited for
+    if (timed_out) {
+        // no new copies were issued after the failed wait; give the ones in
+        // flight a last bounded chance to land before the CTA's shared memory
+        // is released, then report
+        if (tid == 0) {
+            mbar_wait(&bars[0], (unsigned)(nraw - 1) & 1u);
+            mbar_wait(&bars[1], (unsigned)(nmod - 1) & 1u);
+            if (p.err) atomicOr(p.err, 1);
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace ouc

@@ -3,7 +3,8 @@ convolutions, forward and input-gradient passes; FP32 weight gradients)
 against the CPU restatement oracle/cnn.py, which rounds the same operands
 to bfloat16: outputs within 2e-3 and parameter gradients within 2e-2
 relative L2 per layer (the GPU accumulates in FP32 in another order, and an
-activation that lands on a bfloat16 rounding tie may round the other way)."""
+activation that lands on a bfloat16 rounding tie may round the other way).
+The gradient sums are reduced in a fixed order, so they are reproducible."""
 import numpy as np
 import pytest
 
@@ -91,3 +92,30 @@ def test_adam_reduces_a_regression_loss():
         assert net.error() == 0
     print("loss", losses[0], "->", losses[-1])
     assert losses[-1] < 0.5 * losses[0]
+
+
+def test_gradients_are_reproducible():
+    """Weight and bias gradients are reduced in a fixed order (per-block
+    partial sums, then an ordered sum; no atomics): two backward passes on
+    the same inputs give bit-identical gradients, so training runs repeat."""
+    import torch
+    n, H, W = 3, 33, 170
+    rng = np.random.default_rng(5)
+    p = _params(13)
+    x = rng.normal(size=(n, H, W, cnn.DIMS[0][0])).astype(np.float32)
+    gout = rng.normal(size=(n, H, W, 8)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    dx = torch.from_numpy(x).to(dev)
+    dy = torch.empty((n, H, W, 8), dtype=torch.float32, device=dev)
+    dg = torch.from_numpy(gout).to(dev)
+    grads = []
+    with Net(0, p) as net:
+        for _ in range(2):
+            net.zero_grad()
+            net.forward_dev(n, H, W, dx.data_ptr(), dy.data_ptr())
+            net.backward_dev(dg.data_ptr())
+            torch.cuda.synchronize()
+            grads.append(net.grads().copy())
+        assert net.error() == 0
+    assert np.array_equal(grads[0], grads[1])
+    assert np.abs(grads[0]).max() > 0

@@ -104,20 +104,28 @@ def test_snapshot_form_vs_fp64_oracle(c1_fp64, K, prec, comp):
     """The precision form: source snapshots every K imaging levels (scaled
     FP16 or BF16) instead of the backward reconstruction, compensated
     imaging sums, FP64 stack.  The stored forward field is what an exact
-    reconstruction returns, so the reference point is the FP64 oracle with exact strip
-    restore.  Bounds: PP and PS within 1 % below the acquisition zone; over
-    the whole image PP within 1 % and PS within 2 % (the plain FP32 method's
-    whole-image errors, printed above, are larger)."""
+    reconstruction returns, so the reference point is the FP64 oracle with
+    exact strip restore.  Bounds: PP and PS within the 1 % bar below the
+    acquisition zone, and PP within it over the whole image.  Over the whole
+    image PS misses the 1 % bar (about 1.6 %): the same error appears with
+    uncompressed FP32 snapshots of every level, so it is the FP32
+    time-stepping round-off of the direct-wave correlation in the
+    acquisition rows, not the compression -- the FP16 form must stay within
+    0.2 percentage points of that FP32 floor (BF16, with 8 mantissa bits, is
+    printed only)."""
     w, vp, vs, wav, shot, r = c1_fp64
     pp, ps, il, nbytes = _run(w, vp, vs, wav, shot, snapshot_every=K, strip_precision=prec, compensated_image=comp)
     e, e_il = _errors(w, r[o.STRIP_EXACT], pp, ps, il)
     ed = _errors_deep(w, r[o.STRIP_EXACT], pp, ps)
+    fpp, fps, fil, _ = _run(w, vp, vs, wav, shot, snapshot_every=1, strip_precision=o.PREC_FP32)
+    floor, _ = _errors(w, r[o.STRIP_EXACT], fpp, fps, fil)
     print(f"snapshots every {K}, storage {prec}, compensated {comp}: vs FP64 {e}, below row {ACQ_ROWS} {ed}, "
-          f"illumination {e_il:.2e}, device bytes {nbytes / 2**20:.1f} MiB")
+          f"illumination {e_il:.2e}, device bytes {nbytes / 2**20:.1f} MiB; FP32 every-level floor {floor}")
     assert np.isfinite(pp).all() and np.isfinite(ps).all()
     assert worst(ed) <= TOL_PRECISION, ed
     if prec != o.PREC_BF16:
-        assert e["pp"] <= TOL_PRECISION and e["ps"] <= 2 * TOL_PRECISION, e
+        assert e["pp"] <= TOL_PRECISION, e
+        assert e["ps"] <= floor["ps"] + 2e-3, (e, floor)
     assert e_il <= TOL_PRECISION
 
 
