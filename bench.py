@@ -156,14 +156,49 @@ def run_reference(args, rank, world):
     value = statistics.median(vals)
     from ouc_b200 import models
     w = models.c2()
+    ref_cuda = reference_cuda_shot(w)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "grid": [w.cfg.X, w.cfg.Z], "nt": w.cfg.nt, "half_order": w.cfg.half_order},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_cuda": ref_cuda}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_cuda_shot(w):
+    """The reference's own kernels compiled for sm_100a (oracle/_ref, built
+    from its sources by oracle/Makefile with its main()'s launch sequence):
+    one RTM shot of the benchmark grid on this GPU, CUDA events around its
+    forward and backward loops.  None when the build or a GPU is absent."""
+    from oracle.oracle import REF_DIR, Oracle, RefBuild
+    if not os.path.exists(os.path.join(REF_DIR, "libpsref_cuda_c2.so")):
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    cfg = w.cfg
+    L = cfg.npml
+    orc = Oracle()
+    vp = orc.pad(np.pad(w.vp_mig, L), L)
+    vs = orc.pad(np.pad(w.vs_mig, L), L)
+    ax, az = orc.profile(vp, L)
+    src, t0 = orc.ricker(w.fm, cfg.dt, cfg.nt)
+    ref = RefBuild("c2", "cuda")
+    sx = L + w.shots[0].sx
+    f32 = np.float32
+    r = ref.rtm(sx, L + 2, L + 2, t0, f32(cfg.dt), f32(cfg.dx), f32(cfg.dz), vp, vs, ax, az, src)
+    ms = r["ms"][0] + r["ms"][1]
+    cells = cfg.nt * (2 * cfg.X * cfg.Z + cfg.nx * cfg.nz)
+    return {"value": cells / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_shot": ms,
+            "shots_per_hour": 3600.0 / (ms / 1e3),
+            "what": "the reference's kernels (forward_s/forward_u, rt_*, reshot_*, corr_v...) built for sm_100a, "
+                    "one RTM shot of the same grid at a time, CUDA events around its time loops"}
 
 
 def run_survey(args, rank, world):
@@ -260,6 +295,9 @@ def main():
     ap.add_argument("--strips", default="fp32", choices=["fp32", "fp16", "bf16"],
                     help="boundary-strip storage (fp16: scaled per slot and field)")
     ap.add_argument("--compensated", action="store_true", help="compensated FP32 imaging sums")
+    ap.add_argument("--seg-rows", type=int, default=None,
+                    help="step kernel: x-marching segment rows (multiple of 16), 0 for the 32 x 64 tile kernel "
+                         "(default: the library's choice)")
     ap.add_argument("--snapshot-every", type=int, default=0,
                     help="0: reconstruct the source wavefield from boundary strips (the reference's method); "
                          "K: store source snapshots every K imaging levels instead (--strips sets their storage)")
@@ -306,6 +344,8 @@ def main():
     cfg.compensated_image = int(args.compensated)
     cfg.snapshot_every = args.snapshot_every
     mig = o.Context(cfg, w.vp_mig, w.vs_mig, w.rho)
+    if args.seg_rows is not None:
+        mig.set_step_kernel(args.seg_rows)
     stream = torch.cuda.ExternalStream(mig.stream, device=torch.device("cuda", local))
 
     # device-resident inputs
