@@ -14,8 +14,9 @@
 //      columns, with the model rows from the second stage;
 //   3. the U-stage for the own rows [o, o + RB): x-derivatives over S rows
 //      [o - SHX, o + RB + SHX), z-derivatives over the own row;
-//   4. shift: the U rows and S rows the next block needs move up by RB rows
-//      in shared memory (x-windows stay contiguous, no modular indexing).
+//   4. shift: the U rows and S rows the next block needs (2N rows of each,
+//      N of Qxx/Qzx) move up by RB rows in shared memory (x-windows stay
+//      contiguous, no modular indexing).
 // Before the first own block, two prologue iterations load the U rows above
 // the segment and compute the S rows above it (the x-halo of the segment is
 // the only S-stage work done twice).  Between blocks the producer lanes of
@@ -38,12 +39,12 @@ struct MarchGeo {
     static constexpr int TZ = 64;                      // strip width (z)
     static constexpr int RB = 16;                      // rows per block (x)
     static constexpr int NT = kThreads;                // one U-stage float4 per thread
-    static constexpr int SHX = (N + 1) & ~1;           // S rows above/below the own rows
+    static constexpr int SHX = N;                      // S rows above/below the own rows
     static constexpr int HS = (N + 3) & ~3;            // S-stage column halo
     static constexpr int HU = (HS + N + 3) & ~3;       // U column halo
     static constexpr int UC = TZ + 2 * HU;
     static constexpr int SC = TZ + 2 * HS;
-    static constexpr int UR = RB + 2 * (SHX + N);      // U rows held: [o - SHX - N, o + RB + SHX + N)
+    static constexpr int UR = RB + 2 * N;              // U rows held: [o + SHX - N, o + SHX + RB + N)
     static constexpr int SR = RB + 2 * SHX;            // theta, omega, Qxz, Qzz rows: [o - SHX, o + RB + SHX)
     static constexpr int QR = RB + SHX;                // Qxx, Qzx rows: [o, o + RB + SHX)
     static constexpr int oUx = 0;
@@ -64,7 +65,7 @@ struct MarchGeo {
     static constexpr int sItems = (RB / 2) * SCOLS;    // S-stage items: 2 rows x one float4
     static_assert(RB * (TZ / 4) == NT, "one U-stage item per thread");
     static_assert(sItems <= NT, "one S-stage item per thread");
-    static_assert(UR - RB <= NT && SR - RB < RB && QR - RB < RB, "shift geometry");
+    static_assert(UR - RB <= RB && SR - RB <= RB && QR - RB <= RB, "shifts copy disjoint row ranges");
     static_assert((UC * 4) % 16 == 0 && (SC * 4) % 16 == 0, "bulk copies move 16-byte multiples");
 };
 
@@ -261,8 +262,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
                 const int c = 4 * (tid - rp * G::SCOLS) - HS;   // first column, relative to z0
                 const int bs0 = SR - RB + 2 * rp;               // S-buffer row of the first of the two rows
                 const bool ownc = c >= 0 && c < TZ;
-                const float* ux0 = sUx + (bs0 + N) * UC + (c + HU);
-                const float* uz0 = sUz + (bs0 + N) * UC + (c + HU);
+                // U-buffer row of S row bs: (o - SHX + bs) - (o + SHX - N)
+                const float* ux0 = sUx + (bs0 - 2 * SHX + N) * UC + (c + HU);
+                const float* uz0 = sUz + (bs0 - 2 * SHX + N) * UC + (c + HU);
                 float4 exx[2], ezx[2];
                 dx4<N, 2, false>(ux0, UC, a, dvx, exx);   // dvxdx = D-x Ux
                 dx4<N, 2, true>(uz0, UC, a, dvx, ezx);    // dvzdx = D+x Uz
@@ -382,27 +384,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
                 issue_model<N>(p, gm, sbase + RB, z0, sMod, &bars[1], lane);
             }
         }
-        // ---- shift of the U rows: [RB, UR) -> [0, UR - RB) ---------------------------
+        // ---- shift of the U rows: [RB, UR) -> [0, UR - RB) (disjoint ranges; the
+        // S-stage has read them, the next U build writes after the closing barrier)
         {
             constexpr int kCarry = (UR - RB) * G::UCOLS;   // float4s per field
-            constexpr int kPer = (2 * kCarry + kThreads - 1) / kThreads;
-            float4 v[kPer];
-#pragma unroll
-            for (int q = 0; q < kPer; ++q) {
-                const int idx = tid + q * kThreads;
-                if (idx < 2 * kCarry) {
-                    const int f = idx / kCarry, e = idx - f * kCarry;
-                    v[q] = ld4((f ? sUz : sUx) + RB * UC + 4 * e);
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < kPer; ++q) {
-                const int idx = tid + q * kThreads;
-                if (idx < 2 * kCarry) {
-                    const int f = idx / kCarry, e = idx - f * kCarry;
-                    st4((f ? sUz : sUx) + 4 * e, v[q]);
-                }
+            for (int idx = tid; idx < 2 * kCarry; idx += kThreads) {
+                const int f = idx / kCarry, e = idx - f * kCarry;
+                float* u = f ? sUz : sUx;
+                st4(u + 4 * e, ld4(u + RB * UC + 4 * e));
             }
         }
 
