@@ -197,6 +197,10 @@ int group(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture* ap, co
     for (int b = 1; b < n; ++b)
         if ((shots[b].src_type == OUC_SRC_THETA) != theta) return fail(ctx, OUC_EINVAL, "mixed source types in a batch");
     if ((rc = run_backward(ctx, n, ctx->cfg.strip_level == OUC_STRIP_EXACT, theta))) return rc;
+    // runtime stability check of the imaging accumulators (as the whole-grid calls do)
+    for (int b = 0; b < n; ++b)
+        launch_finite_check(ctx->acc[0] - (size_t)kGX * ctx->pitch - kZOFF + (size_t)b * ctx->shot_stride,
+                            3 * ctx->fstride, ctx->d_status, ctx->stream);
     CKS(cudaEventRecord(ctx->ev[2], ctx->stream));
     // normalisation + Laplacian per shot, into the stack at the shot's rows
     const size_t ni = (size_t)ctx->nx * ctx->nz;
@@ -215,6 +219,7 @@ int group(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture* ap, co
             f.stack[k] = ctx->d_stack[k] + (size_t)ap[b].x0 * ctx->nz;
         }
         f.img = ctx->d_img + (size_t)(2 * b) * ni;
+        f.status = ctx->d_status;
         launch_finalize(f, ctx->stream);
         ctx->timing.kernel_launches += 1;
     }
@@ -225,6 +230,7 @@ int group(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture* ap, co
     }
     CKS(cudaEventRecord(ctx->ev[3], ctx->stream));
     CKS(cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_status(ctx))) return rc;
     ctx->timing.forward_ms += elapsed(ctx->ev[0], ctx->ev[1]);
     ctx->timing.backward_ms += elapsed(ctx->ev[1], ctx->ev[2]);
     ctx->timing.finalize_ms += elapsed(ctx->ev[2], ctx->ev[3]);

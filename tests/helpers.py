@@ -59,3 +59,20 @@ def golden_shot(g, mute=1):
     import ouc_b200 as o
     L = int(g["L"])
     return o.Shot(sx=int(g["sx"]) - L, sz=int(g["sz"]) - L, rz=int(g["rz"]) - L, t0=int(g["t0"]), mute=mute)
+
+
+def strip_bytes_fp64(cfg):
+    """Host bytes of the FP64 oracle's boundary strips for one RTM shot of
+    `cfg` (8 fields of the 2N-wide bands around the interior, every step)."""
+    N, X, Z = cfg.half_order, cfg.nx + 2 * cfg.npml, cfg.nz + 2 * cfg.npml
+    return 8 * 8 * (cfg.nt - 1) * 2 * 2 * N * (X + Z)
+
+
+def require_host_memory(nbytes, factor=4):
+    """Skip the test unless the host has `factor` x nbytes of memory available
+    (the FP64 oracle of a long shot keeps large strip arrays)."""
+    import psutil
+    import pytest
+    avail = psutil.virtual_memory().available
+    if avail < factor * nbytes:
+        pytest.skip(f"needs {factor * nbytes / 2**30:.0f} GiB of host memory, {avail / 2**30:.0f} GiB available")

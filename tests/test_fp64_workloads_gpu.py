@@ -13,7 +13,9 @@ configurations themselves (not only on the small golden grids).
   the whole pipeline in FP64 (its records are rounded to float32, the input
   precision of the migration).
 
-The FP64 run of the headline shot takes one to three minutes of host time.
+The FP64 run of the headline shot takes one to three minutes of host time and
+keeps about 8 GB of boundary strips in host memory (skipped without four
+times that available).
 Bounds: gathers 1e-5 (the FP32 floor the golden grids show).  The fields'
 bound is the FP32 floor of the reference's own arithmetic on the same run:
 the oracle's float instantiation (the reference's kernels' operation order,
@@ -31,7 +33,7 @@ import numpy as np
 import pytest
 
 import ouc_b200 as o
-from helpers import finite_rel_l2, rel_l2
+from helpers import finite_rel_l2, rel_l2, require_host_memory, strip_bytes_fp64
 from oracle.oracle import Oracle, Shot
 
 pytestmark = pytest.mark.gpu
@@ -118,6 +120,7 @@ def test_headline_rtm_shot_vs_fp64_oracle():
         pp, ps = ctx.rtm_shot(shot, wav, rec=(gx, gz))
     sh = Shot(X=cfg.X, Z=cfg.Z, L=L, N=cfg.half_order, nt=cfg.nt, sx=L + s.sx, sz=L + s.sz, rz=L + s.rz,
               dx=cfg.dx, dz=cfg.dz, dt=cfg.dt, t0=t0)
+    require_host_memory(strip_bytes_fp64(cfg))
     vpt, vst, axt, azt = _padded(orc, w.vp, w.vs, L)
     gx64, gz64, _ = orc.forward(sh, vpt, vst, axt, azt, wav, fp64=True)
     vpm, vsm, axm, azm = _padded(orc, w.vp_mig, w.vs_mig, L)
