@@ -311,8 +311,8 @@ int ouc_tune(ouc_ctx* ctx, int steps, int* best_batch, int* best_seg_rows, float
  * in 16-row blocks with bulk asynchronous row copies; 0: one CTA per 32 x 64
  * tile.  Both replace the reference's per-step kernel pair (forward_s +
  * forward_u, PS:316-384 / PS:205-314, and their receiver and reconstruction
- * twins) with bit-identical results.  ouc_create picks about 192 rows;
- * ouc_tune_batch times the candidates.  Changing it drops the captured time
+ * twins) with bit-identical results.  ouc_create picks the tile kernel;
+ * ouc_tune times both geometries.  Changing it drops the captured time
  * loops (they are captured again on next use). */
 int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows);
 int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows);

@@ -63,14 +63,6 @@ int check_status(ouc_ctx* ctx) {
     return fail(ctx, OUC_EUNSTABLE, "non-finite wavefield (unstable run: check the CFL number and the inputs)");
 }
 
-// Rows per x-marching segment by default: about 192 (a multiple of 16), so
-// that a segment's S-stage halo (twice the stencil's row halo) stays a few
-// per cent of its work while a batch still spreads over several waves.
-int default_seg_rows(int X) {
-    const int nseg = std::max(1, (X + 191) / 192);
-    const int rows = (X + nseg - 1) / nseg;
-    return std::max(64, (rows + 15) / 16 * 16);
-}
 
 // Edge padding of the interior model into the absorbing layer, as the
 // reference's xiangbian (PS:37-119): sides copy the nearest interior
@@ -766,7 +758,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     cudaMemsetAsync(ctx->model, 0, model_bytes, ctx->stream);
     cudaMemsetAsync(ctx->state, 0, state_bytes, ctx->stream);
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
-    ctx->seg_rows = default_seg_rows(ctx->X);
+    ctx->seg_rows = 0;   // the tile kernel; ouc_tune / ouc_set_step_kernel choose the march
     for (int q = 0; q < 3; ++q) cudaMemsetAsync(ctx->d_stack[q], 0, ni * 8, ctx->stream);
     ctx->vp2 = ctx->field(ctx->model, 0); ctx->vs2 = ctx->field(ctx->model, 1);
     ctx->ax = ctx->field(ctx->model, 2); ctx->az = ctx->field(ctx->model, 3);

@@ -79,22 +79,22 @@ __device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ bool mbar_test(uint64_t* b, unsigned parity) {
+// One hardware-suspended wait on phase `parity`: the thread sleeps until the
+// phase completes or a time limit of about 0.1 ms passes (no busy polling).
+__device__ __forceinline__ bool mbar_try(uint64_t* b, unsigned parity) {
     unsigned ok;
     asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n}"
         : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity)
+        : "r"(smem_u32(b)), "r"(parity), "r"(100000u)
         : "memory");
     return ok != 0;
 }
-// Bounded wait on phase `parity`: false after about 20 ms of polling (a row
-// copy takes microseconds).
+// Bounded wait on phase `parity`: false after about 200 suspended tries
+// (some 20 ms; a row copy takes microseconds).
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
-    for (int k = 0; k < (1 << 17); ++k) {
-        if (mbar_test(b, parity)) return true;
-        if (k >= 32) __nanosleep(128);
-    }
+    for (int k = 0; k < 200; ++k)
+        if (mbar_try(b, parity)) return true;
     return false;
 }
 // One contiguous global -> shared copy (16-byte aligned, 16-byte multiple),

@@ -116,4 +116,4 @@ def test_step_kernel_rejects_bad_segments():
         for bad in (-16, 8, 20):
             with pytest.raises(o.OucError):
                 ctx.set_step_kernel(bad)
-        assert ctx.step_kernel() % 16 == 0 and ctx.step_kernel() > 0   # the default is the march
+        assert ctx.step_kernel() == 0   # the default is the tile kernel (measured faster); tuning may pick the march
