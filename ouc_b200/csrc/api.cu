@@ -364,10 +364,11 @@ StepArgs rec_args(const ouc_ctx* ctx) {
 
 // Receiver side at time t: record injection + S/U stages with damping
 // (PS:2319-2324, 2349-2354).
-int rcv_step(ouc_ctx* ctx, StepArgs& ar, Side& r, int n, int t) {
+int rcv_step(ouc_ctx* ctx, StepArgs& ar, Side& r, int n, int t, cudaStream_t st = nullptr) {
     bind_side(ar, r);
     ar.t = t;
-    if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+    if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, n, st ? st : ctx->stream))
+        return fail(ctx, OUC_EINVAL, "no kernel for N");
     r.swap_levels();
     r.swap_memory();
     ctx->timing.kernel_launches += 1;
@@ -436,11 +437,33 @@ int run_backward_loop(ouc_ctx* ctx, int n, bool exact_strips, bool theta_src) {
     if (ctx->cfg.gradient) CK(cudaMemsetAsync(ctx->grad, 0, (size_t)n * 3 * ctx->fstride * sizeof(float), ctx->stream));
     StepArgs ar = rcv_args(ctx);
     StepArgs as = rec_args(ctx);
-    for (int t = ctx->nt - 1; t >= 0; --t) {
-        if ((rc = rcv_step(ctx, ar, r, n, t))) return rc;
-        if (ctx->cfg.gradient) grad_step(ctx, s, r, n, t);
-        if ((rc = rec_step(ctx, as, s, r, n, t, exact_strips, theta_src))) return rc;
+    if (ctx->cfg.gradient || !ctx->stream2) {
+        for (int t = ctx->nt - 1; t >= 0; --t) {
+            if ((rc = rcv_step(ctx, ar, r, n, t))) return rc;
+            if (ctx->cfg.gradient) grad_step(ctx, s, r, n, t);
+            if ((rc = rec_step(ctx, as, s, r, n, t, exact_strips, theta_src))) return rc;
+        }
+        CK(cudaGetLastError());
+        return OUC_OK;
     }
+    // Two streams, so that the reconstruction of step t overlaps the
+    // receiver step t-1: rec(t) reads the receiver level rcv(t) wrote and
+    // rcv(t-1) only reads it too (it writes the older buffer), so the two are
+    // independent; rcv(t-2) overwrites that level and waits for rec(t).  The
+    // source side stays in order on the context stream.  Same launches, same
+    // arguments, same results as the serial loop.
+    cudaStream_t sr = ctx->stream2;
+    CK(cudaEventRecord(ctx->evb[0], ctx->stream));   // the receiver stream starts after the work queued so far
+    CK(cudaStreamWaitEvent(sr, ctx->evb[0], 0));
+    for (int t = ctx->nt - 1; t >= 0; --t) {
+        if (t <= ctx->nt - 3) CK(cudaStreamWaitEvent(sr, ctx->evb[1 + (t & 1)], 0));   // rec(t+2) is done
+        if ((rc = rcv_step(ctx, ar, r, n, t, sr))) return rc;
+        CK(cudaEventRecord(ctx->evb[0], sr));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->evb[0], 0));                          // rcv(t) is done
+        if ((rc = rec_step(ctx, as, s, r, n, t, exact_strips, theta_src))) return rc;
+        CK(cudaEventRecord(ctx->evb[1 + (t & 1)], ctx->stream));
+    }
+    // rec(0) waited for rcv(0), the receiver stream's last work: joined
     CK(cudaGetLastError());
     return OUC_OK;
 }
@@ -705,6 +728,10 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         ctx->own_stream = true;
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
+    // second stream and ordering events of the overlapped backward loop
+    if (cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess) return bad("cannot create stream", OUC_ECUDA);
+    for (auto& e : ctx->evb)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return bad("cannot create events", OUC_ECUDA);
 
     // layout
     const int TX = 32, TZ = 64;
@@ -810,6 +837,8 @@ int ouc_destroy(ouc_ctx* ctx) {
     for (auto* p : ctx->d_gstack) cudaFree(p);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->evb) if (e) cudaEventDestroy(e);
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return OUC_OK;

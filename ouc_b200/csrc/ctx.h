@@ -104,6 +104,8 @@ struct ouc_ctx {
     float* fo_sq = nullptr;
     size_t bytes = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t stream2 = nullptr;    // receiver steps of the overlapped backward loop
+    cudaEvent_t evb[3] = {nullptr, nullptr, nullptr};   // its ordering events (no timing)
 
     // step-level interface: one shot (slot 0) advanced one launch per call
     enum { kIdle, kForward, kReceiver, kReconstruct, kFinalize } step_phase = kIdle;
