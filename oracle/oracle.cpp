@@ -581,6 +581,88 @@ struct Engine {
         if (fields_out) dump_fields(wr, fields_out);
     }
 
+    // RTM with the source wavefield stored during the forward pass instead of
+    // reconstructed from boundary strips (the library's snapshot form): the
+    // source P displacement of every K-th imaging level is kept (interior
+    // only) and correlated with the receiver side there.  Imaging steps are
+    // t = nt-1, nt-1-K, ...; step t uses the new level of forward step t
+    // (exact alignment, and t = nt-1) or t+1 (the reference's alignment,
+    // PS:964 + PS:2361).  No reconstruction, so no round-off amplification
+    // by the inverse leapfrog: the reference point for long runs.
+    void rtm_stored(const float* src, const float* rec_in_x, const float* rec_in_z, int K, T* lap_pp, T* lap_ps,
+                    T* acc) {
+        const int nt = cfg.nt, nx = X - 2 * L, nz = Z - 2 * L;
+        std::vector<int> slot_of(nt, -1), slot_at(nt, -1);   // forward step -> slot, backward step -> slot
+        int nslots = 0;
+        for (int t = nt - 1; t >= 0; t -= K) {
+            const int f = (cfg.image_align == 1 || t == nt - 1) ? t : t + 1;
+            if (slot_of[f] < 0) slot_of[f] = nslots++;
+            slot_at[t] = slot_of[f];
+        }
+        const size_t ci = (size_t)nx * nz;
+        std::vector<T> store((size_t)nslots * 2 * ci);
+        Wave<T> ws, wr;
+        ws.init(X, Z); wr.init(X, Z);
+        std::vector<T> rvx((size_t)X * nt, T(0)), rvz((size_t)X * nt, T(0));
+        const bool theta = cfg.src_type == 0;
+        for (int f = 0; f < nt; ++f) {
+            stage_s(ws, f, src, theta);
+            stage_u(ws);
+            if (!theta) force(ws, src, f);
+            record(ws, rvx.data(), rvz.data(), f);
+            if (slot_of[f] >= 0) {
+                T* d = store.data() + (size_t)slot_of[f] * 2 * ci;
+#pragma omp parallel for schedule(static)
+                for (int i = 0; i < nx; ++i)
+                    for (int j = 0; j < nz; ++j) {
+                        d[(size_t)i * nz + j] = ws.pnx(i + L, j + L);
+                        d[ci + (size_t)i * nz + j] = ws.pnz(i + L, j + L);
+                    }
+            }
+        }
+        if (rec_in_x)
+            for (size_t k = 0; k < rvx.size(); ++k) { rvx[k] = (T)rec_in_x[k]; rvz[k] = (T)rec_in_z[k]; }
+        if (cfg.do_mute) mute(rvx.data(), rvz.data());
+        Field<T> numpp, numps, den;
+        numpp.init(X, Z); numps.init(X, Z); den.init(X, Z);
+        for (int t = nt - 1; t >= 0; --t) {
+            inject(wr, rvx.data(), rvz.data(), t);
+            stage_s(wr, t, src, false);
+            stage_u(wr);
+            if (slot_at[t] < 0) continue;
+            const T* d = store.data() + (size_t)slot_at[t] * 2 * ci;
+#pragma omp parallel for schedule(static)
+            for (int i = L; i < X - L; ++i)
+                for (int j = L; j < Z - L; ++j) {
+                    const size_t o = (size_t)(i - L) * nz + (j - L);
+                    const T px = d[o], pz = d[ci + o];
+                    numpp(i, j) += px * wr.pnx(i, j) + pz * wr.pnz(i, j);
+                    den(i, j) += px * px + pz * pz;
+                    numps(i, j) += px * wr.snx(i, j) + pz * wr.snz(i, j);
+                }
+        }
+        const T dh = (T)cfg.dx;
+        for (int i = L; i < X - L; ++i)
+            for (int j = L; j < Z - L; ++j) {
+                T vpp = 0, vps = 0;
+                if (i >= L + 2 && i < X - L - 2 && j >= L + 2 && j < Z - L - 2) {
+                    auto ip = [&](int a, int b) { return numpp(a, b) / den(a, b); };
+                    auto is = [&](int a, int b) { return numps(a, b) / den(a, b); };
+                    vpp = (1 / dh / dh) * (ip(i + 1, j) + ip(i - 1, j) - 2 * ip(i, j) + ip(i, j + 1) + ip(i, j - 1) - 2 * ip(i, j));
+                    vps = (1 / dh / dh) * (is(i + 1, j) + is(i - 1, j) - 2 * is(i, j) + is(i, j + 1) + is(i, j - 1) - 2 * is(i, j));
+                }
+                const size_t o = (size_t)(i - L) * nz + (j - L);
+                lap_pp[o] = vpp;
+                lap_ps[o] = vps;
+            }
+        if (acc) {
+            const size_t C = (size_t)X * Z;
+            std::copy(numpp.v.begin(), numpp.v.end(), acc);
+            std::copy(numps.v.begin(), numps.v.end(), acc + C);
+            std::copy(den.v.begin(), den.v.end(), acc + 2 * C);
+        }
+    }
+
     // 12 fields in a fixed order: ux uz Px Pz Sx Sz th om qzx qzz qxx qxz
     static void dump_fields(Wave<T>& w, T* out) {
         Field<T>* fs[12] = {&w.ux, &w.uz, &w.pnx, &w.pnz, &w.snx, &w.snz, &w.th, &w.om, &w.qzx, &w.qzz, &w.qxx, &w.qxz};
@@ -771,6 +853,18 @@ int orc_rtm_f64(const orc_cfg* c, const float* vp, const float* vs, const float*
     Engine<double> e;
     e.setup(c, vp, vs, ax, az);
     e.rtm(src, rec_x, rec_z, lap_pp, lap_ps, raw_pp, raw_ps, acc, rec_out, fields_out);
+    return 0;
+}
+
+// RTM from the stored source wavefield (Engine::rtm_stored), every K-th
+// imaging level, in double precision: the FP64 reference of the snapshot form.
+int orc_rtm_stored_f64(const orc_cfg* c, const float* vp, const float* vs, const float* ax, const float* az,
+                       const float* src, const float* rec_x, const float* rec_z, int K, double* lap_pp,
+                       double* lap_ps, double* acc) {
+    if (K < 1) return 1;
+    Engine<double> e;
+    e.setup(c, vp, vs, ax, az);
+    e.rtm_stored(src, rec_x, rec_z, K, lap_pp, lap_ps, acc);
     return 0;
 }
 

@@ -127,6 +127,9 @@ class Oracle:
         self.lib.orc_pad_model.argtypes = [_fp, C.c_int, C.c_int, C.c_int]
         self.lib.orc_cpml_profile.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_double, _fp, _fp]
         self.lib.orc_num_threads.restype = C.c_int
+        self.lib.orc_rtm_stored_f64.argtypes = [C.POINTER(OrcCfg), _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _dp, _dp,
+                                                _dp]
+        self.lib.orc_rtm_stored_f64.restype = C.c_int
         self.lib.orc_ricker.argtypes = [C.c_float, C.c_float, C.c_int, _fp, C.POINTER(C.c_int)]
         self.lib.orc_ricker.restype = C.c_int
         self.lib.orc_set_threads.argtypes = [C.c_int]
@@ -206,6 +209,24 @@ class Oracle:
                _ptr(np.ascontiguousarray(rec_vz, np.float32)), _ptr(fields, dt))
         assert rc == 0
         return fields
+
+    def rtm_stored(self, shot: Shot, vp, vs, ax, az, src, every=1, rec=None):
+        """FP64 RTM from the stored source wavefield of every `every`-th imaging
+        level (no reconstruction): the reference of the snapshot form.  Keeps
+        nt/every x 2 x nx x nz doubles."""
+        X, Z, nt, L = shot.X, shot.Z, shot.nt, shot.L
+        nx, nz = X - 2 * L, Z - 2 * L
+        out = dict(lap_pp=np.zeros((nx, nz)), lap_ps=np.zeros((nx, nz)), acc=np.zeros((3, X, Z)))
+        rx = rz = None
+        if rec is not None:
+            rx = np.ascontiguousarray(rec[0], dtype=np.float32)
+            rz = np.ascontiguousarray(rec[1], dtype=np.float32)
+        c = shot.cfg()
+        rc = self.lib.orc_rtm_stored_f64(C.byref(c), _ptr(vp), _ptr(vs), _ptr(ax), _ptr(az), _ptr(src), _ptr(rx),
+                                         _ptr(rz), int(every), _ptr(out["lap_pp"], np.float64),
+                                         _ptr(out["lap_ps"], np.float64), _ptr(out["acc"], np.float64))
+        assert rc == 0
+        return out
 
     def rtm(self, shot: Shot, vp, vs, ax, az, src, rec=None, fp64=False, rho=None):
         """rho (padded density): the variable-density extension, FP64 only."""

@@ -16,7 +16,9 @@ configurations themselves (not only on the small golden grids).
 The FP64 run of the headline shot takes one to three minutes of host time and
 keeps about 8 GB of boundary strips in host memory (skipped without four
 times that available).
-Bounds: gathers 1e-5 (the FP32 floor the golden grids show).  The fields'
+Bounds: gathers 1e-5 (the FP32 floor the golden grids show) or, for the
+4000-step headline shot, twice the reference arithmetic's own FP32 floor
+there (about 1e-5).  The fields'
 bound is the FP32 floor of the reference's own arithmetic on the same run:
 the oracle's float instantiation (the reference's kernels' operation order,
 bit-exact against them on the CPU) against its double instantiation.  After
@@ -125,10 +127,13 @@ def test_headline_rtm_shot_vs_fp64_oracle():
     require_host_memory(strip_bytes_fp64(cfg))
     vpt, vst, axt, azt = _padded(orc, w.vp, w.vs, L)
     gx64, gz64, _ = orc.forward(sh, vpt, vst, axt, azt, wav, fp64=True)
+    gx32, gz32, _ = orc.forward(sh, vpt, vst, axt, azt, wav)   # the reference arithmetic in FP32
+    floor = max(rel_l2(gx32, gx64), rel_l2(gz32, gz64))
     vpm, vsm, axm, azm = _padded(orc, w.vp_mig, w.vs_mig, L)
     r = orc.rtm(sh, vpm, vsm, axm, azm, wav, rec=(gx64, gz64), fp64=True)
     e = {"gather_vx": rel_l2(gx, gx64), "gather_vz": rel_l2(gz, gz64),
          "image_pp": finite_rel_l2(pp, r["lap_pp"]), "image_ps": finite_rel_l2(ps, r["lap_ps"])}
-    print("headline RTM shot (1000 x 500, nt = 4000): FP32 CUDA vs FP64 oracle", e)
-    assert max(e["gather_vx"], e["gather_vz"]) <= TOL_GATHER, e
+    print("headline RTM shot (1000 x 500, nt = 4000): FP32 CUDA vs FP64 oracle", e,
+          "reference-arithmetic FP32 gather floor", floor)
+    assert max(e["gather_vx"], e["gather_vz"]) <= max(2.0 * floor, TOL_GATHER), (e, floor)
     assert max(e["image_pp"], e["image_ps"]) <= TOL_IMAGE_C2, e
