@@ -419,44 +419,6 @@ __device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, 
     }
 }
 
-// L2 prefetch of the damping-layer operands of a tile that meets the layers
-// (uniform flags): the S-stage CPML memories and profile over the S region,
-// the U-stage memories over the own cells -- the loads that follow the
-// derivatives would otherwise wait for DRAM in those tiles.
-template <int N, int MODE>
-__device__ __forceinline__ void prefetch_damping(const StepArgs& p, const Geo& gm, size_t off, int x0, int z0, bool px,
-                                                 bool pz) {
-    using G = TileGeo<N>;
-    constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS;
-    if (MODE == kRec || !(px || pz)) return;
-    const int tid = threadIdx.x;
-    const int P = p.pitch;
-    constexpr int kSPer = (TZ + 2 * HS + 31) / 32 + 1;
-    constexpr int kSLines = (TX + 2 * SHX) * kSPer;
-    // S region: f_old xx, zx and ax (px); f_old zz, xz and az (pz)
-    for (int k = tid; k < 3 * kSLines; k += kThreads) {
-        const int f = k / kSLines, l = k - f * kSLines;
-        const int g = (x0 - SHX + l / kSPer) * P + (z0 - HS) + 32 * (l % kSPer);
-        if (px) {
-            const float* a = f == 0 ? p.f_old[0] + off : f == 1 ? p.f_old[3] + off : gm.ax;
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(a + g));
-        }
-        if (pz) {
-            const float* a = f == 0 ? p.f_old[1] + off : f == 1 ? p.f_old[2] + off : gm.az;
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(a + g));
-        }
-    }
-    // own cells: the U-stage memories E, B, Tx, Wx (px) and C, A, Tz, Wz (pz)
-    constexpr int kOwnLines = TX * (TZ / 32);
-    for (int k = tid; k < 4 * kOwnLines; k += kThreads) {
-        const int f = k / kOwnLines, l = k - f * kOwnLines;
-        const int g = (x0 + l / (TZ / 32)) * P + z0 + 32 * (l % (TZ / 32));
-        constexpr int ox[4] = {1, 2, 4, 7}, oz[4] = {0, 3, 5, 6};
-        if (px) asm volatile("prefetch.global.L2 [%0];" ::"l"(p.o[ox[f]] + off + g));
-        if (pz) asm volatile("prefetch.global.L2 [%0];" ::"l"(p.o[oz[f]] + off + g));
-    }
-}
-
 // Offsets within one field are 32-bit ints (row * pitch + column, guard rows
 // negative): ouc_create refuses grids whose field allocation exceeds 2^31
 // floats, and the 32-bit multiply-adds are fewer instructions than the
@@ -874,7 +836,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
     prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
     const ShotView sv = shot_view(p, blockIdx.y);
     const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
-    prefetch_damping<N, MODE>(p, gm, d.off, x0, z0, f.px, f.pz);
     step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f);
 }
 
