@@ -296,8 +296,8 @@ def main():
                     help="boundary-strip storage (fp16: scaled per slot and field)")
     ap.add_argument("--compensated", action="store_true", help="compensated FP32 imaging sums")
     ap.add_argument("--seg-rows", type=int, default=None,
-                    help="step kernel: x-marching segment rows (multiple of 16), 0 for the 32 x 64 tile kernel "
-                         "(default: the library's choice)")
+                    help="step kernel: x-marching segment rows (multiple of 16), 0 for the 32 x 64 tile kernel, "
+                         "-1 for the tile kernel with a dynamic tile queue (default: the library's choice)")
     ap.add_argument("--snapshot-every", type=int, default=0,
                     help="0: reconstruct the source wavefield from boundary strips (the reference's method); "
                          "K: store source snapshots every K imaging levels instead (--strips sets their storage)")
@@ -441,8 +441,9 @@ def main():
            "receiver": (56 * C + damp + 8 * X) * B,
            "reconstruction": (80 * Ci + 8 * ring_cells(cfg) * sb) * B}
     seg = mig.step_kernel()
-    kname = (lambda m: f"k_march<{cfg.half_order}, {m}> ({seg}-row segments, 16-row blocks)" if seg else
-             f"k_step<{cfg.half_order}, {m}> (32 x 64 tiles)")
+    kname = (lambda m: f"k_march<{cfg.half_order}, {m}> ({seg}-row segments, 16-row blocks)" if seg > 0 else
+             f"k_step_q<{cfg.half_order}, {m}> (32 x 64 tiles, persistent launch with a dynamic tile queue)" if seg < 0
+             else f"k_step<{cfg.half_order}, {m}> (32 x 64 tiles)")
     kern = {}
     if not args.snapshot_every:
         iso = mig.time_step_kernels(B, reps=20)

@@ -309,11 +309,14 @@ int ouc_tune(ouc_ctx* ctx, int steps, int* best_batch, int* best_seg_rows, float
 /* Step-kernel geometry.  seg_rows > 0 (a multiple of 16): the x-marching
  * kernel, each CTA walking a 64-column strip down a segment of that many rows
  * in 16-row blocks with bulk asynchronous row copies; 0: one CTA per 32 x 64
- * tile.  Both replace the reference's per-step kernel pair (forward_s +
+ * tile; OUC_STEP_TILE_QUEUE: the tile kernel as a persistent launch (two
+ * CTAs per SM) claiming (tile, shot) items from a dynamic queue, heaviest
+ * tiles (damping layers, boundary ring) first.  All replace the reference's per-step kernel pair (forward_s +
  * forward_u, PS:316-384 / PS:205-314, and their receiver and reconstruction
  * twins) with bit-identical results.  ouc_create picks the tile kernel;
  * ouc_tune times both geometries.  Changing it drops the captured time
  * loops (they are captured again on next use). */
+#define OUC_STEP_TILE_QUEUE (-1)
 int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows);
 int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows);
 

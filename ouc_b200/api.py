@@ -22,6 +22,7 @@ IMAGE_REFERENCE, IMAGE_EXACT = 0, 1
 PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
 SRC_THETA, SRC_FORCE_Z = 0, 1
 GATHER_XT, GATHER_TX = 0, 1
+STEP_TILE_QUEUE = -1
 
 
 @dataclass
@@ -367,8 +368,10 @@ class Context:
         return gp, gs, il
 
     def set_step_kernel(self, seg_rows):
-        """Step-kernel geometry: x-marching segments of seg_rows rows (a
-        multiple of 16), or 0 for the 32 x 64 tile kernel (ouc_set_step_kernel)."""
+        """Step-kernel geometry (ouc_set_step_kernel): 0 the 32 x 64 tile
+        kernel, STEP_TILE_QUEUE (-1) the tile kernel as a persistent launch
+        with a dynamic tile queue, or x-marching segments of seg_rows rows
+        (a multiple of 16)."""
         check(lib().ouc_set_step_kernel(self._h, int(seg_rows)), self._h)
 
     def time_step_kernels(self, n, reps=10):

@@ -52,6 +52,37 @@ int cuda_fail(ouc_ctx* c, cudaError_t e, const char* what) {
 
 // Read and clear the context's device status word after a synchronising call:
 // a bounded copy wait that gave up, or a non-finite wavefield.
+// Tile orders of the dynamic-queue form, heaviest first: tiles whose S
+// region meets the damping layers (CPML memories to read and write) and
+// tiles that meet the boundary ring (strips to save or restore) lead, then
+// the interior tiles; ties in row-major order.  Entries are tx << 16 | tz,
+// relative to the launch's tile origin.
+std::vector<int> tile_order(const ouc_ctx* ctx, bool rec) {
+    const int TX = 32, TZ = 64, SHX = (ctx->N + 1) & ~1, HS = (ctx->N + 3) & ~3;
+    const int nx = rec ? ctx->rec_tiles_x : ctx->tiles_x, nz = rec ? ctx->rec_tiles_z : ctx->tiles_z;
+    const int tx0 = rec ? ctx->rec_tx0 : 0, tz0 = rec ? ctx->rec_tz0 : 0;
+    const int X = ctx->X, Z = ctx->Z, L = ctx->L;
+    std::vector<std::pair<int, int>> w;
+    for (int tx = 0; tx < nx; ++tx)
+        for (int tz = 0; tz < nz; ++tz) {
+            const int x0 = (tx0 + tx) * TX, z0 = (tz0 + tz) * TZ;
+            int weight = 0;
+            if (!rec && (x0 - SHX < L || x0 + TX + SHX - 1 >= X - L)) weight += 2;
+            if (!rec && (z0 - HS < L || z0 + TZ + HS - 1 >= Z - L)) weight += 2;
+            const Ring& R = ctx->ring;
+            const bool meets_box = x0 - 2 * R.N < X - L + R.N && x0 + TX + 2 * R.N > L - R.N &&
+                                   z0 - 2 * R.N < Z - L + R.N && z0 + TZ + 2 * R.N > L - R.N;
+            const bool deep = x0 - 2 * R.N >= L + R.N && x0 + TX + 2 * R.N <= X - L - R.N &&
+                              z0 - 2 * R.N >= L + R.N && z0 + TZ + 2 * R.N <= Z - L - R.N;
+            if (meets_box && !deep) weight += 1;
+            w.push_back({-weight, tx * nz + tz});
+        }
+    std::stable_sort(w.begin(), w.end());
+    std::vector<int> out;
+    for (auto& e : w) out.push_back(((e.second / nz) << 16) | (e.second % nz));
+    return out;
+}
+
 int check_status(ouc_ctx* ctx) {
     int st = 0;
     CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -129,6 +160,10 @@ StepArgs base_args(const ouc_ctx* c) {
     a.density = c->cfg.density;
     a.seg_rows = c->seg_rows;
     a.err = c->d_status;
+    a.nsm = c->nsm;
+    a.queue = c->d_queue;
+    a.order[0] = c->d_order[0];
+    a.order[1] = c->d_order[1];
     for (int k = 0; k < 3; ++k) a.comp[k] = c->comp[k];
     a.ring = c->ring;
     a.shots = c->d_desc;
@@ -773,6 +808,9 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
               cudaMalloc(&ctx->d_img, 2 * ni * ctx->batch * 4) == cudaSuccess &&
               cudaMalloc(&ctx->d_desc, ctx->batch * sizeof(ShotDesc)) == cudaSuccess &&
               cudaMalloc(&ctx->d_status, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_queue, 6 * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_order[0], (size_t)ctx->tiles_x * ctx->tiles_z * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_order[1], (size_t)ctx->rec_tiles_x * ctx->rec_tiles_z * sizeof(int)) == cudaSuccess &&
               cudaMalloc(&ctx->d_stack[0], ni * 8) == cudaSuccess && cudaMalloc(&ctx->d_stack[1], ni * 8) == cudaSuccess &&
               cudaMalloc(&ctx->d_stack[2], ni * 8) == cudaSuccess;
     if (!ok) {
@@ -785,6 +823,14 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     cudaMemsetAsync(ctx->model, 0, model_bytes, ctx->stream);
     cudaMemsetAsync(ctx->state, 0, state_bytes, ctx->stream);
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+    cudaMemsetAsync(ctx->d_queue, 0, 6 * sizeof(int), ctx->stream);
+    {
+        const std::vector<int> o0 = tile_order(ctx, false), o1 = tile_order(ctx, true);
+        cudaMemcpyAsync(ctx->d_order[0], o0.data(), o0.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(ctx->d_order[1], o1.data(), o1.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);   // the host vectors go out of scope
+    }
+    cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
     ctx->seg_rows = 0;   // the tile kernel; ouc_tune / ouc_set_step_kernel choose the march
     for (int q = 0; q < 3; ++q) cudaMemsetAsync(ctx->d_stack[q], 0, ni * 8, ctx->stream);
     ctx->vp2 = ctx->field(ctx->model, 0); ctx->vs2 = ctx->field(ctx->model, 1);
@@ -829,6 +875,7 @@ int ouc_destroy(ouc_ctx* ctx) {
     cudaFree(ctx->model); cudaFree(ctx->state);
     cudaFree(ctx->gathers); cudaFree(ctx->staging); cudaFree(ctx->d_wavelet);
     cudaFree(ctx->d_img); cudaFree(ctx->d_desc); cudaFree(ctx->d_status);
+    cudaFree(ctx->d_queue); cudaFree(ctx->d_order[0]); cudaFree(ctx->d_order[1]);
     for (auto* p : ctx->d_stack) cudaFree(p);
     cudaFree(ctx->strips); cudaFree(ctx->stage); cudaFree(ctx->amax);
     cudaFree(ctx->snaps); cudaFree(ctx->snap_amax);
@@ -846,8 +893,8 @@ int ouc_destroy(ouc_ctx* ctx) {
 
 int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows) {
     if (!ctx) return OUC_EINVAL;
-    if (seg_rows != 0 && (seg_rows < 16 || seg_rows % 16 != 0))
-        return fail(ctx, OUC_EINVAL, "segment rows must be 0 (tiles) or a positive multiple of 16");
+    if (seg_rows != 0 && seg_rows != OUC_STEP_TILE_QUEUE && (seg_rows < 16 || seg_rows % 16 != 0))
+        return fail(ctx, OUC_EINVAL, "segment rows must be 0 (tiles), OUC_STEP_TILE_QUEUE or a positive multiple of 16");
     if (seg_rows == ctx->seg_rows) return OUC_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);

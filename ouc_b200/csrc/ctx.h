@@ -41,6 +41,9 @@ struct ouc_ctx {
     int run_batch = 1;           // shots advanced per launch (<= batch; ouc_tune_batch)
     int seg_rows = 0;            // step kernel: x-marching segments of this many rows, or 0 for 32 x 64 tiles
     int* d_status = nullptr;     // device status word: bit 0 a copy wait timed out, bit 1 a non-finite field
+    int nsm = 148;               // SMs of the device
+    int* d_queue = nullptr;      // dynamic-queue form: [mode][claim counter, finished CTAs]
+    int* d_order[2] = {nullptr, nullptr};   // its tile orders, heaviest first: full grid, reconstruction
     size_t fstride = 0;          // floats per field allocation
     size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;

@@ -839,4 +839,54 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
     step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f);
 }
 
+// The same step as a persistent launch with a dynamic work queue: a few
+// CTAs per SM claim (tile, shot) items from a device counter until the
+// queue is empty.  Items are ordered heaviest first -- the tiles that meet
+// the damping layers (CPML memories) and the boundary ring (strips) lead,
+// per the host-built table p.order -- so the cheap interior tiles fill the
+// end of the launch.  Each CTA claims its next item while it works on the
+// current one and prefetches that tile's operands to L2 right after it has
+// its index.  The last CTA to finish resets the counters for the next
+// launch of the same mode (no memset per launch).  No waits: a CTA only
+// atomically increments the counter and reads its value.
+template <int N, int MODE>
+__global__ void __launch_bounds__(kThreads, 2) k_step_q(const StepArgs p, int nshots, int ntiles) {
+    extern __shared__ float4 smem4[];
+    float* sm = reinterpret_cast<float*>(smem4);
+    __shared__ int s_item[2];
+    using G = TileGeo<N>;
+    int* counter = p.queue + 2 * MODE;
+    int* done = counter + 1;
+    const int* order = p.order[MODE == kRec ? 1 : 0];
+    const int nitems = ntiles * nshots;
+    if (threadIdx.x == 0) s_item[0] = atomicAdd(counter, 1);
+    __syncthreads();
+    int item = s_item[0], buf = 0;
+    while (item < nitems) {
+        if (threadIdx.x == 0) s_item[buf ^ 1] = atomicAdd(counter, 1);
+        const int b = item % nshots, k = item / nshots;
+        const int tx = order[k] >> 16, tz = order[k] & 0xffff;
+        const ShotDesc& d = p.shots[b];
+        if (tx < (MODE == kRec ? d.rec_tiles_x : d.tiles_x)) {   // within this shot's width
+            const int x0 = (p.tile_x0 + tx) * G::TX, z0 = (p.tile_z0 + tz) * G::TZ;
+            const Geo gm = geo_of(d);
+            prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
+            const ShotView sv = shot_view(p, b);
+            const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
+            step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f);
+        }
+        __syncthreads();   // the tile's shared memory is free and the next index is visible
+        item = s_item[buf ^ 1];
+        buf ^= 1;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();   // this CTA's claims are complete before it counts itself done
+        if (atomicAdd(done, 1) == (int)gridDim.x - 1) {
+            *counter = 0;
+            *done = 0;
+            __threadfence();
+        }
+    }
+}
+
 }  // namespace ouc

@@ -18,6 +18,11 @@ static cudaError_t configure_one() {
         e = cudaFuncSetAttribute(k_step<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_step_q<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TileGeo<N>::bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_step_q<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_march<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, MarchGeo<N>::bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_march<N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -55,6 +60,12 @@ static void launch_one(const StepArgs& a, int tiles_x, int nshots, cudaStream_t 
     if (a.seg_rows > 0) {
         const int nseg = march_segments((Mode)MODE, a);
         k_march<N, MODE><<<dim3(nseg * a.tiles_z, nshots), kThreads, MarchGeo<N>::bytes, s>>>(a);
+        return;
+    }
+    if (a.seg_rows < 0 && a.queue && a.order[MODE == kRec ? 1 : 0]) {
+        const int ntiles = tiles_x * a.tiles_z;
+        const int items = ntiles * nshots, grid = items < 2 * a.nsm ? items : 2 * a.nsm;
+        k_step_q<N, MODE><<<grid, kThreads, TileGeo<N>::bytes, s>>>(a, nshots, ntiles);
         return;
     }
     constexpr int bytes = TileGeo<N>::bytes;

@@ -127,7 +127,11 @@ struct StepArgs {
     int strip_prec;                   // StripPrec of the strips
     int comp_image;                   // kRec: compensated (Kahan) imaging sums, comp[] below
     int density;                      // variable density: scale the U-stage by the buoyancy
-    int seg_rows;                     // > 0: the x-marching kernel, segments of this many rows (a multiple of 16)
+    int seg_rows;                     // > 0: the x-marching kernel, segments of this many rows (a multiple of 16);
+                                      // 0: one CTA per 32 x 64 tile; -1: the tile kernel with a dynamic queue
+    int nsm;                          // SMs of the device (persistent grid of the queue form)
+    int* queue;                       // queue form: [mode][claim counter, finished CTAs], zero between launches
+    const int* order[2];              // queue form: tiles (tx << 16 | tz), heaviest first: full grid, reconstruction
     int* err;                         // device word: kernels record OUC_ETIMEOUT-class failures here (or null)
     float a[6];                       // stencil weights a_1..a_N
     float dx, dz, dt, dt2;

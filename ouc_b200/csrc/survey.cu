@@ -319,7 +319,7 @@ int ouc_tune(ouc_ctx* ctx, int steps, int* best_batch, int* best_seg_rows, float
     cudaSetDevice(ctx->device);
     ctx->step_phase = ouc_ctx::kIdle;
     if (cudaMemsetAsync(ctx->d_wavelet, 0, (size_t)ctx->nt * 4, ctx->stream) != cudaSuccess) return OUC_ECUDA;
-    std::vector<int> batches, segs = {0};
+    std::vector<int> batches, segs = {0, OUC_STEP_TILE_QUEUE};
     for (int n = 1; n < ctx->batch; n *= 2) batches.push_back(n);
     batches.push_back(ctx->batch);
     for (int r : {64, 96, 128, 192, 256, 384, 512})

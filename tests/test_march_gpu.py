@@ -1,4 +1,5 @@
-"""The x-marching step kernel against the 32 x 64 tile kernel.
+"""The x-marching step kernel and the dynamic-queue (persistent) launch of
+the tile kernel against the 32 x 64 tile kernel.
 
 Both kernels implement the same fused time step (the reference's forward_s +
 forward_u pair, PS:316-384 / PS:205-314, and its receiver and reconstruction
@@ -18,7 +19,8 @@ from helpers import CASES, golden_shot, load_golden, make_context
 
 pytestmark = pytest.mark.gpu
 
-SEGS = [16, 48, 128, 4096]
+QUEUE = -1          # OUC_STEP_TILE_QUEUE
+SEGS = [QUEUE, 16, 48, 128, 4096]
 
 
 def _run(g, seg, shots=None, **over):
@@ -61,7 +63,9 @@ def test_march_equals_tiles_in_every_form(over):
         s = golden_shot(g)
         s.sx = sx
         shots.append(s)
-    _same(_run(g, 48, shots, **over), _run(g, 0, shots, **over))
+    ref = _run(g, 0, shots, **over)
+    _same(_run(g, 48, shots, **over), ref)
+    _same(_run(g, QUEUE, shots, **over), ref)
 
 
 def test_march_equals_tiles_force_source_and_density():
@@ -70,7 +74,7 @@ def test_march_equals_tiles_force_source_and_density():
     X, Z = int(g["X"]), int(g["Z"])
     rho = np.linspace(1800, 2600, (X - 2 * L) * (Z - 2 * L)).reshape(X - 2 * L, Z - 2 * L).astype(np.float32)
     res = []
-    for seg in (0, 32):
+    for seg in (0, 32, QUEUE):
         sh = golden_shot(g)
         sh.src_type = o.SRC_FORCE_Z
         with make_context(g) as ctx:
@@ -82,9 +86,10 @@ def test_march_equals_tiles_force_source_and_density():
             ctx.set_step_kernel(seg)
             res.append(ctx.forward(golden_shot(g), g["src"], fields=True))
             res.append(ctx.rtm_shot(golden_shot(g), g["src"]))
-    for a, b in zip(res[:3], res[3:]):
-        for x, y in zip(a, b):
-            assert np.array_equal(x, y, equal_nan=True)
+    for other in (res[3:6], res[6:9]):
+        for a, b in zip(res[:3], other):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y, equal_nan=True)
 
 
 def test_march_equals_tiles_on_a_survey():
@@ -95,25 +100,26 @@ def test_march_equals_tiles_on_a_survey():
     shots = [o.Shot(40, 2, 2, t0=t0), o.Shot(150, 2, 2, t0=t0), o.Shot(260, 2, 2, t0=t0)]
     aps = [(0, 120), (60, 250), (150, 300)]
     out = []
-    for seg in (0, 64):
+    for seg in (0, 64, QUEUE):
         with o.Context(cfg, vp, vs) as ctx:
             ctx.set_step_kernel(seg)
             recs = ctx.survey_forward(shots, aps, wav)
             imgs = ctx.survey_rtm(shots, aps, wav, recs)
             out.append((recs, imgs, ctx.stack()))
-    (r0, i0, s0), (r1, i1, s1) = out
-    for a, b in zip(r0, r1):
-        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-    for a, b in zip(i0, i1):
-        assert np.array_equal(a[0], b[0], equal_nan=True) and np.array_equal(a[1], b[1], equal_nan=True)
-    for a, b in zip(s0, s1):
-        assert np.array_equal(a, b, equal_nan=True)
+    r0, i0, s0 = out[0]
+    for r1, i1, s1 in out[1:]:
+        for a, b in zip(r0, r1):
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        for a, b in zip(i0, i1):
+            assert np.array_equal(a[0], b[0], equal_nan=True) and np.array_equal(a[1], b[1], equal_nan=True)
+        for a, b in zip(s0, s1):
+            assert np.array_equal(a, b, equal_nan=True)
 
 
 def test_step_kernel_rejects_bad_segments():
     g = load_golden("g64n6")
     with make_context(g) as ctx:
-        for bad in (-16, 8, 20):
+        for bad in (-16, -2, 8, 20):
             with pytest.raises(o.OucError):
                 ctx.set_step_kernel(bad)
         assert ctx.step_kernel() == 0   # the default is the tile kernel (measured faster); tuning may pick the march
