@@ -60,12 +60,12 @@ int cuda_fail(ouc_ctx* c, cudaError_t e, const char* what) {
 std::vector<int> tile_order(const ouc_ctx* ctx, bool rec) {
     const int TX = 32, TZ = 64, SHX = (ctx->N + 1) & ~1, HS = (ctx->N + 3) & ~3;
     const int nx = rec ? ctx->rec_tiles_x : ctx->tiles_x, nz = rec ? ctx->rec_tiles_z : ctx->tiles_z;
-    const int tx0 = rec ? ctx->rec_tx0 : 0, tz0 = rec ? ctx->rec_tz0 : 0;
+    const int ox = rec ? ctx->rec_x0 : 0, oz = rec ? ctx->rec_z0 : 0;
     const int X = ctx->X, Z = ctx->Z, L = ctx->L;
     std::vector<std::pair<int, int>> w;
     for (int tx = 0; tx < nx; ++tx)
         for (int tz = 0; tz < nz; ++tz) {
-            const int x0 = (tx0 + tx) * TX, z0 = (tz0 + tz) * TZ;
+            const int x0 = ox + tx * TX, z0 = oz + tz * TZ;
             int weight = 0;
             if (!rec && (x0 - SHX < L || x0 + TX + SHX - 1 >= X - L)) weight += 2;
             if (!rec && (z0 - HS < L || z0 + TZ + HS - 1 >= Z - L)) weight += 2;
@@ -391,7 +391,7 @@ StepArgs rcv_args(const ouc_ctx* ctx) { return base_args(ctx); }
 
 StepArgs rec_args(const ouc_ctx* ctx) {
     StepArgs as = base_args(ctx);
-    as.tiles_z = ctx->rec_tiles_z; as.tile_x0 = ctx->rec_tx0; as.tile_z0 = ctx->rec_tz0;
+    as.tiles_z = ctx->rec_tiles_z; as.tile_x0 = ctx->rec_x0; as.tile_z0 = ctx->rec_z0;
     as.img_past = ctx->cfg.image_align == OUC_IMAGE_REFERENCE;
     for (int k = 0; k < 3; ++k) as.acc[k] = ctx->acc[k];
     return as;
@@ -661,8 +661,9 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     {   // one field (guard rows and columns, padded to whole tiles) must stay
         // below 2^31 cells: the kernels address within a field with 32-bit offsets
         const long long Xp = (long long)cfg->nx + 2LL * L, Zp = (long long)cfg->nz + 2LL * L;
-        const long long rows = (Xp + 31) / 32 * 32 + 2LL * kGX;
-        const long long pitch = ((Zp + 63) / 64 * 64 + 2LL * kZOFF + 31) / 32 * 32;
+        // (bounds of TileGrid's Xc, Zc: one more tile row and column)
+        const long long rows = (Xp + 31) / 32 * 32 + 32 + 2LL * kGX;
+        const long long pitch = ((Zp + 63) / 64 * 64 + 64 + 2LL * kZOFF + 31) / 32 * 32;
         if (rows * pitch > (long long)INT_MAX) return bad("grid too large: one field would exceed 2^31 cells");
     }
     if (cfg->strip_precision != OUC_PREC_FP32 && cfg->strip_precision != OUC_PREC_FP16 &&
@@ -769,15 +770,14 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return bad("cannot create events", OUC_ECUDA);
 
     // layout
-    const int TX = 32, TZ = 64;
-    ctx->tiles_x = (X + TX - 1) / TX; ctx->tiles_z = (Z + TZ - 1) / TZ;
-    ctx->Xc = ctx->tiles_x * TX; ctx->Zc = ctx->tiles_z * TZ;
+    const TileGrid tg = tile_grid(X, Z, L);
+    ctx->tiles_x = tg.tiles_x; ctx->tiles_z = tg.tiles_z;
+    ctx->Xc = tg.Xc; ctx->Zc = tg.Zc;
     ctx->pitch = ((kZOFF + ctx->Zc + kZOFF) + 31) / 32 * 32;
     ctx->fstride = (size_t)(ctx->Xc + 2 * kGX) * ctx->pitch;   // < 2^31 (checked above)
     ctx->shot_stride = (size_t)kFieldsPerShot * ctx->fstride;
-    ctx->rec_tx0 = L / TX; ctx->rec_tz0 = L / TZ;
-    ctx->rec_tiles_x = (X - L - 1) / TX - ctx->rec_tx0 + 1;
-    ctx->rec_tiles_z = (Z - L - 1) / TZ - ctx->rec_tz0 + 1;
+    ctx->rec_x0 = tg.rec_x0; ctx->rec_z0 = tg.rec_z0;
+    ctx->rec_tiles_x = tg.rec_tiles_x; ctx->rec_tiles_z = tg.rec_tiles_z;
     ctx->ring = Ring::make(X, Z, L, N);
     ctx->strip_slot = (size_t)kStripFields * ctx->ring.R;
     if (cfg->snapshot_every > 0) {

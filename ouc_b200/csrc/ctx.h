@@ -47,7 +47,7 @@ struct ouc_ctx {
     size_t fstride = 0;          // floats per field allocation
     size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;
-    int rec_tx0 = 0, rec_tz0 = 0, rec_tiles_x = 0, rec_tiles_z = 0;
+    int rec_x0 = 0, rec_z0 = 0, rec_tiles_x = 0, rec_tiles_z = 0;   // reconstruction tiles (TileGrid)
     float a[6] = {0, 0, 0, 0, 0, 0};
     cudaStream_t stream = nullptr;
     bool own_stream = false;

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
     if (xs >= row_end) return;   // beyond this shot's rows
     if (p.err && (*(volatile int*)p.err & 1)) return;   // an earlier copy wait gave up: do nothing more
     const int xe = min(xs + p.seg_rows, row_end);
-    const int z0 = (p.tile_z0 + strip) * TZ;
+    const int z0 = p.tile_z0 + strip * TZ;
     const int nblk = (xe - xs + RB - 1) / RB;
     const Geo gm = geo_of(d);
     const ShotView sv = shot_view(p, blockIdx.y);

@@ -400,10 +400,12 @@ __device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, 
         const int g = (ux_i0 + l / kUPer) * P + ux_j0 + 32 * (l % kUPer);
         asm volatile("prefetch.global.L2 [%0];" ::"l"(p.now[f] + off + g));
     }
-    constexpr int kOwnLines = TX * (TZ / 32);
+    // own rows: TZ / 32 + 1 lines, as the tile need not start on a line
+    constexpr int kOwnPer = TZ / 32 + 1;
+    constexpr int kOwnLines = TX * kOwnPer;
     for (int k = tid; k < 4 * kOwnLines; k += kThreads) {
         const int f = k / kOwnLines, l = k - f * kOwnLines;
-        const int g = (x0 + l / (TZ / 32)) * P + z0 + 32 * (l % (TZ / 32));
+        const int g = (x0 + l / kOwnPer) * P + z0 + 32 * (l % kOwnPer);
         asm volatile("prefetch.global.L2 [%0];" ::"l"(p.past[f] + off + g));
         if (MODE == kRec) {
             asm volatile("prefetch.global.L2 [%0];" ::"l"(p.rcv[f] + off + g));
@@ -448,11 +450,33 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
     const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;   // global origin of the U box
 
     // ---- phase 1: U = P + S over the tile and a 2N halo ---------------------
-    for (int idx = tid; idx < G::UR * (UC / 4); idx += kThreads) {
-        const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
-        const int g = (ux_i0 + r) * P + (ux_j0 + 4 * c4);
-        st4(sUx + r * UC + 4 * c4, add4(ld4(nowp[0] + g), ld4(nowp[2] + g)));   // Ux = Px + Sx (PS:302)
-        st4(sUz + r * UC + 4 * c4, add4(ld4(nowp[1] + g), ld4(nowp[3] + g)));
+    // Every load of the thread's share of the box (at most 6 rounds of four
+    // float4) is issued before any is used, so that all of them are in flight
+    // at once (2 % faster than a load-add-store loop at c2).
+    {
+        constexpr int kBox = G::UR * (UC / 4);
+        constexpr int kRounds = (kBox + kThreads - 1) / kThreads;
+        static_assert(kRounds <= 6, "U box loads held in registers");
+        float4 v[kRounds][4];
+#pragma unroll
+        for (int q = 0; q < kRounds; ++q) {
+            const int idx = tid + q * kThreads;
+            if (idx < kBox) {
+                const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
+                const int g = (ux_i0 + r) * P + (ux_j0 + 4 * c4);
+#pragma unroll
+                for (int fld = 0; fld < 4; ++fld) v[q][fld] = ld4(nowp[fld] + g);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kRounds; ++q) {
+            const int idx = tid + q * kThreads;
+            if (idx < kBox) {
+                const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
+                st4(sUx + r * UC + 4 * c4, add4(v[q][0], v[q][2]));   // Ux = Px + Sx (PS:302)
+                st4(sUz + r * UC + 4 * c4, add4(v[q][1], v[q][3]));
+            }
+        }
     }
     if (MODE == kRcv && f.inj) {
         __syncthreads();
@@ -831,7 +855,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
     const ShotDesc& d = p.shots[blockIdx.y];
     if ((int)blockIdx.x >= (MODE == kRec ? d.rec_tiles_x : d.tiles_x) * p.tiles_z) return;   // beyond this shot's width
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
-    const int x0 = (p.tile_x0 + tx) * G::TX, z0 = (p.tile_z0 + tz) * G::TZ;
+    const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
     const Geo gm = geo_of(d);
     prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
     const ShotView sv = shot_view(p, blockIdx.y);
@@ -868,7 +892,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_q(const StepArgs p, int ns
         const int tx = order[k] >> 16, tz = order[k] & 0xffff;
         const ShotDesc& d = p.shots[b];
         if (tx < (MODE == kRec ? d.rec_tiles_x : d.tiles_x)) {   // within this shot's width
-            const int x0 = (p.tile_x0 + tx) * G::TX, z0 = (p.tile_z0 + tz) * G::TZ;
+            const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
             const Geo gm = geo_of(d);
             prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
             const ShotView sv = shot_view(p, b);

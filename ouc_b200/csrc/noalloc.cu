@@ -131,9 +131,9 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
 
     // layout: the same pitched padded grid as ouc_create
     const int X = cfg->nx + 2 * L, Z = cfg->nz + 2 * L, nt = cfg->nt;
-    const int TX = 32, TZ = 64;
-    const int tiles_x = (X + TX - 1) / TX, tiles_z = (Z + TZ - 1) / TZ;
-    const int Xc = tiles_x * TX, Zc = tiles_z * TZ;
+    const TileGrid tg = tile_grid(X, Z, L);
+    const int tiles_x = tg.tiles_x, tiles_z = tg.tiles_z;
+    const int Xc = tg.Xc, Zc = tg.Zc;
     const int pitch = ((kZOFF + Zc + kZOFF) + 31) / 32 * 32;
     const size_t fstride = (size_t)(Xc + 2 * kGX) * pitch;
     const size_t nfields = 4 + 24;   // model: vp2 vs2 ax az; state: now 4, past 4, F 2x4, O 8

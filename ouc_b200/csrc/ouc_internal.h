@@ -23,6 +23,34 @@ constexpr int kGX = 16;        // guard rows on each side
 constexpr int kZOFF = 16;      // guard columns on each side
 constexpr int kThreads = 256;  // threads per step CTA
 
+// Tile grids of the step kernels (32 x 64 cell tiles).  The forward and
+// receiver steps tile the padded grid from (0, 0).  The reconstruction
+// updates only the interior [L, X-L) x [L, Z-L), so its tiles start at
+// x = L and z = L rounded down to a multiple of 4 (float4 alignment): at
+// 1000 x 500 with L = 30 that is 32 x 8 tiles instead of the 33 x 9 that
+// tiles from the origin would need.  Xc x Zc is the extent the field
+// allocations hold (before their guard rows and columns) so that every
+// tile's cells lie inside.
+struct TileGrid {
+    int tiles_x, tiles_z;          // full step, from (0, 0)
+    int rec_x0, rec_z0;            // reconstruction: cell origin of its first tile
+    int rec_tiles_x, rec_tiles_z;
+    int Xc, Zc;
+};
+inline int rec_tiles_for(int X, int L) { return (X - 2 * L + 31) / 32; }
+inline TileGrid tile_grid(int X, int Z, int L) {
+    TileGrid g;
+    g.tiles_x = (X + 31) / 32;
+    g.tiles_z = (Z + 63) / 64;
+    g.rec_x0 = L;
+    g.rec_z0 = L & ~3;
+    g.rec_tiles_x = rec_tiles_for(X, L);
+    g.rec_tiles_z = (Z - L - g.rec_z0 + 63) / 64;
+    g.Xc = g.tiles_x * 32 > g.rec_x0 + g.rec_tiles_x * 32 ? g.tiles_x * 32 : g.rec_x0 + g.rec_tiles_x * 32;
+    g.Zc = g.tiles_z * 64 > g.rec_z0 + g.rec_tiles_z * 64 ? g.tiles_z * 64 : g.rec_z0 + g.rec_tiles_z * 64;
+    return g;
+}
+
 // Float32 staggered weights a_1..a_N by half-order N (row N).  N = 6: the
 // reference's literals (PS:221).  Other N: the exact Taylor solution of
 // sum_k c_k (2k-1)^(2n-1) = [n==1], rounded to float32 where used.  The one
@@ -118,7 +146,7 @@ struct ShotDesc {
 
 struct StepArgs {
     int X, Z, pitch, L;
-    int tiles_z, tile_x0, tile_z0;    // tile grid of this launch
+    int tiles_z, tile_x0, tile_z0;    // tile columns of this launch; cell origin of its first tile
     int t;                            // time step index
     int slot_u, slot_s;               // kRec: strip slots holding U and theta..Qxz at level t+1
     int record, save;                 // kFwd: write gathers / boundary strips this step

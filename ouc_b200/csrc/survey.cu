@@ -117,7 +117,7 @@ int upload_batch(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture*
         s.amax = ctx->amax ? ctx->amax + (size_t)b * ctx->nt * kStripFields : nullptr;
         s.X = w.X;
         s.tiles_x = (w.X + TX - 1) / TX;
-        s.rec_tiles_x = (w.X - L - 1) / TX - ctx->rec_tx0 + 1;
+        s.rec_tiles_x = rec_tiles_for(w.X, L);
         s.ring = Ring::make(w.X, Z, L, ctx->N);
         s.off = (size_t)b * ctx->shot_stride;
         s.strip_slot = ctx->strip_slot;
