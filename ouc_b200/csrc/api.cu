@@ -167,6 +167,10 @@ StepArgs base_args(const ouc_ctx* c) {
     for (int k = 0; k < 3; ++k) a.comp[k] = c->comp[k];
     a.ring = c->ring;
     a.shots = c->d_desc;
+    a.box_map = c->box_map;
+    a.state0 = c->box_state0;
+    a.fstride = c->fstride;
+    a.nfields = kFieldsPerShot;
     return a;
 }
 
@@ -277,6 +281,7 @@ int upload_desc(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_wavel
         d[b].rec_tiles_x = ctx->rec_tiles_x;
         d[b].ring = ctx->ring;
         d[b].off = (size_t)b * ctx->shot_stride;
+        d[b].slot = b;
         d[b].strip_slot = ctx->strip_slot;
         d[b].vp2 = ctx->vp2; d[b].vs2 = ctx->vs2; d[b].ax = ctx->ax; d[b].az = ctx->az;
         d[b].bx = ctx->bx; d[b].bz = ctx->bz;
@@ -304,7 +309,8 @@ int zero_side(ouc_ctx* ctx, int n, int side, bool with_acc) {
 int fwd_step(ouc_ctx* ctx, StepArgs& a, Side& s, int n, int t) {
     bind_side(a, s);
     a.t = t;
-    if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+    if (launch_step(ctx->N, kFwd, a, ctx->tiles_x, n, ctx->stream))
+        return fail(ctx, OUC_EINVAL, "step launch refused (half-order or state map)");
     s.swap_levels();
     s.swap_memory();
     ctx->timing.kernel_launches += 1;
@@ -403,7 +409,7 @@ int rcv_step(ouc_ctx* ctx, StepArgs& ar, Side& r, int n, int t, cudaStream_t st 
     bind_side(ar, r);
     ar.t = t;
     if (launch_step(ctx->N, kRcv, ar, ctx->tiles_x, n, st ? st : ctx->stream))
-        return fail(ctx, OUC_EINVAL, "no kernel for N");
+        return fail(ctx, OUC_EINVAL, "step launch refused (half-order or state map)");
     r.swap_levels();
     r.swap_memory();
     ctx->timing.kernel_launches += 1;
@@ -431,7 +437,8 @@ int rec_step(ouc_ctx* ctx, StepArgs& as, Side& s, const Side& r, int n, int t, b
     as.slot_u = exact_strips ? t : (t + 1 == nt - 1 ? nt - 2 : t + 1);
     as.slot_s = t + 1;
     for (int k = 0; k < 4; ++k) as.rcv[k] = r.now[k];
-    if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, n, ctx->stream)) return fail(ctx, OUC_EINVAL, "no kernel for N");
+    if (launch_step(ctx->N, kRec, as, ctx->rec_tiles_x, n, ctx->stream))
+        return fail(ctx, OUC_EINVAL, "step launch refused (half-order or state map)");
     s.swap_levels();
     ctx->timing.kernel_launches += 1;
     return OUC_OK;
@@ -850,6 +857,15 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
     for (int q = 0; q < 3; ++q) ctx->comp[q] = ctx->field(ctx->state, k++);
     ctx->src0 = ctx->src;
     ctx->rcv0 = ctx->rcv;
+    {   // the state block's tensor map (U boxes of the step kernels)
+        StepArgs m;
+        memset(&m, 0, sizeof(m));
+        if (encode_box_map(m, ctx->state, ctx->pitch, ctx->Xc + 2 * kGX, kFieldsPerShot, ctx->batch, ctx->fstride, N) !=
+            cudaSuccess)
+            return bad("cannot encode the state block's tensor map", OUC_ECUDA);
+        ctx->box_map = m.box_map;
+        ctx->box_state0 = m.state0;
+    }
     // kernel attributes set before any graph capture
     if (configure_step_kernels(N) != cudaSuccess) {
         cudaGetLastError();

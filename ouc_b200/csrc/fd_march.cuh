@@ -69,34 +69,7 @@ struct MarchGeo {
     static_assert((UC * 4) % 16 == 0 && (SC * 4) % 16 == 0, "bulk copies move 16-byte multiples");
 };
 
-// ---- bulk asynchronous copies and mbarriers ----------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-// One hardware-suspended wait on phase `parity`: the thread sleeps until the
-// phase completes or a time limit of about 0.1 ms passes (no busy polling).
-__device__ __forceinline__ bool mbar_try(uint64_t* b, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity), "r"(100000u)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait on phase `parity`: false after about 200 suspended tries
-// (some 20 ms; a row copy takes microseconds).
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
-    for (int k = 0; k < 200; ++k)
-        if (mbar_try(b, parity)) return true;
-    return false;
-}
+// ---- untiled bulk copies (the mbarrier helpers are in fd_step.cuh) ----------
 // One contiguous global -> shared copy (16-byte aligned, 16-byte multiple),
 // completing `bytes` of the mbarrier's transaction count.  No multicast.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* b) {
@@ -105,7 +78,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  "l"(src), "r"(bytes), "r"(smem_u32(b))
                  : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Issue the raw-stage copies of iteration k (U rows [base, base + RB), the
 // four P/S fields of the current level, columns [z0 - HU, z0 + TZ + HU)) from

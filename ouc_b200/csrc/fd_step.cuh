@@ -6,8 +6,9 @@
 // HBM arrays (forward_s then forward_u, PS:2261-2264; rt_s_res/rt_u_res;
 // reshot_u/reshot_s).  Here each CTA owns a TX x TZ tile of one shot
 // (blockIdx.y = shot) and, in three phases separated by __syncthreads():
-//   1. loads the total displacement U = P + S of its tile plus a 2N halo into
-//      shared memory (float4 loads along the contiguous z axis);
+//   1. brings the P and S fields of its tile plus a 2N halo into shared
+//      memory by tensor copies (cp.async.bulk.tensor boxes completing on an
+//      mbarrier, bounded wait) and sums them to the total displacement U;
 //   2. computes the S-stage (theta, omega and the four Q fields, with the
 //      S-stage CPML memory) for its tile plus an N halo, keeping it on chip:
 //      halo cells are recomputed by both neighbouring CTAs, so the six
@@ -40,6 +41,8 @@
 // IEEE division on sm_100a for the spacings in use); quotients near the
 // subnormal range go through double precision (div4 below).
 #pragma once
+#include <cstdint>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -191,6 +194,46 @@ __device__ __forceinline__ void dx4(const float* col, int st, const float* a, co
         out[q] = div4(cat4(acl, ach), dv);
     }
 }
+
+// ---- bulk asynchronous copies and mbarriers ----------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+// One hardware-suspended wait on phase `parity`: the thread sleeps until the
+// phase completes or a time limit of about 0.1 ms passes (no busy polling).
+__device__ __forceinline__ bool mbar_try(uint64_t* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity), "r"(100000u)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on phase `parity`: false after about 200 suspended tries
+// (some 20 ms; a tile's copies take microseconds).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+    for (int k = 0; k < 200; ++k)
+        if (mbar_try(b, parity)) return true;
+    return false;
+}
+// One box of a 4-D tensor map (tile mode, no multicast) into shared memory
+// at `dst` (128-byte aligned), completing its bytes on the mbarrier.  The
+// innermost coordinate c0 must be a multiple of 4 (16 bytes of floats).
+__device__ __forceinline__ void tma_box4(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(b))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Per-launch, per-shot constants.
 struct ShotView {
@@ -379,27 +422,20 @@ __device__ __forceinline__ bool u_live(const StepArgs& p, const Geo& gm, int gi,
     return gi >= N && gi < gm.X - N && gj >= N && gj < p.Z - N;
 }
 
-// L2 prefetch of a tile's operands, one 128-byte line per instruction, so
-// that the loads of the three phases find their lines in flight or resident:
-// the U box of phase 1 (current level, 4 fields), the oldest level (read and
-// overwritten in phase 3) and, for the reconstruction, the receiver level and
-// the imaging accumulators over the own cells, and the model over the S
-// region (phase 2).  Every address lies inside the field allocations (guard
-// rows and columns included).
+// L2 prefetch of a tile's thread-loaded operands, one 128-byte line per
+// instruction, so that the loads of phases 2 and 3 find their lines in
+// flight or resident: the oldest level (read and overwritten in phase 3)
+// and, for the reconstruction, the receiver level and the imaging
+// accumulators over the own cells, and the model over the S region
+// (phase 2).  (The U box of phase 1 arrives by tensor copies.)  Every
+// address lies inside the field allocations (guard rows and columns
+// included).
 template <int N, int MODE>
 __device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, size_t off, int x0, int z0) {
     using G = TileGeo<N>;
-    constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS, HU = G::HU;
+    constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS;
     const int tid = threadIdx.x;
     const int P = p.pitch;
-    const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;
-    constexpr int kUPer = (G::UC + 16 + 31) / 32;   // the box starts 16 floats into a line
-    constexpr int kULines = G::UR * kUPer;
-    for (int k = tid; k < 4 * kULines; k += kThreads) {
-        const int f = k / kULines, l = k - f * kULines;
-        const int g = (ux_i0 + l / kUPer) * P + ux_j0 + 32 * (l % kUPer);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(p.now[f] + off + g));
-    }
     // own rows: TZ / 32 + 1 lines, as the tile need not start on a line
     constexpr int kOwnPer = TZ / 32 + 1;
     constexpr int kOwnLines = TX * kOwnPer;
@@ -425,9 +461,14 @@ __device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, 
 // negative): ouc_create refuses grids whose field allocation exceeds 2^31
 // floats, and the 32-bit multiply-adds are fewer instructions than the
 // 64-bit ones (+1.3 % measured).
+// One tile's step.  `bar` is the CTA's mbarrier (initialised, count 1) and
+// `parity` the phase that this tile's copies complete.  Returns false, with
+// bit 0 of *p.err set, when the copies did not land within the wait's bound
+// (or an earlier launch had recorded such a failure): the tile is then left
+// unwritten and the host reports OUC_ETIMEOUT after the call.
 template <int N, int MODE>
-__device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, const ShotView& sv, float* sm, int x0, int z0,
-                                          const TileFlags& f) {
+__device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, const ShotView& sv, float* sm, int x0, int z0,
+                                          const TileFlags& f, uint64_t* bar, unsigned parity) {
     using G = TileGeo<N>;
     constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS, HU = G::HU, UC = G::UC, SC = G::SC;
     const int tid = threadIdx.x;
@@ -450,33 +491,41 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
     const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;   // global origin of the U box
 
     // ---- phase 1: U = P + S over the tile and a 2N halo ---------------------
-    // Every load of the thread's share of the box (at most 6 rounds of four
-    // float4) is issued before any is used, so that all of them are in flight
-    // at once (2 % faster than a load-add-store loop at c2).
-    {
-        constexpr int kBox = G::UR * (UC / 4);
-        constexpr int kRounds = (kBox + kThreads - 1) / kThreads;
-        static_assert(kRounds <= 6, "U box loads held in registers");
-        float4 v[kRounds][4];
-#pragma unroll
-        for (int q = 0; q < kRounds; ++q) {
-            const int idx = tid + q * kThreads;
-            if (idx < kBox) {
-                const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
-                const int g = (ux_i0 + r) * P + (ux_j0 + 4 * c4);
-#pragma unroll
-                for (int fld = 0; fld < 4; ++fld) v[q][fld] = ld4(nowp[fld] + g);
-            }
+    // One thread issues four tensor copies (cp.async.bulk.tensor, the UC x
+    // UR box of each P/S field of the current level, completing on the CTA's
+    // mbarrier): P into the U arrays, S into the S-stage area, which is
+    // unused until phase 2.  The whole 83 KB box is in flight at once and no
+    // thread holds it in registers.  One shared-memory pass then adds S to P.
+    float* stS = sm + G::oTh;   // Sx then Sz staging, UR x UC each
+    static_assert(G::floats - G::oTh >= 2 * G::UR * UC, "S staging fits the S-stage area");
+    static_assert((G::oUz * 4) % 128 == 0 && (G::oTh * 4) % 128 == 0 && (G::UR * UC * 4) % 128 == 0,
+                  "tensor-copy destinations are 128-byte aligned");
+    const int err_word = p.err ? *(volatile const int*)p.err : 0;   // consumed after the wait
+    if (tid == 0) {
+        mbar_arrive_tx(bar, 4u * G::UR * UC * 4u);
+        // the previous tile's shared-memory accesses (generic proxy) precede these writes
+        fence_proxy_async();
+        // allocation coordinates: column ux_j0 + kZOFF (a multiple of 4), row ux_i0 + kGX (>= 0)
+        const int c0 = ux_j0 + kZOFF, c1 = ux_i0 + kGX, slot = p.shots[sv.b].slot;
+        tma_box4(sUx, &p.box_map, c0, c1, p.now_field[0], slot, bar);
+        tma_box4(sUz, &p.box_map, c0, c1, p.now_field[1], slot, bar);
+        tma_box4(stS, &p.box_map, c0, c1, p.now_field[2], slot, bar);
+        tma_box4(stS + G::UR * UC, &p.box_map, c0, c1, p.now_field[3], slot, bar);
+    }
+    const bool landed = mbar_wait(bar, parity);
+    if (!__syncthreads_and(landed && !(err_word & 1))) {
+        // a failed wait: one more bounded wait lets copies in flight land
+        // before the shared memory is reused or released; then report
+        if (tid == 0) {
+            if (!landed) mbar_wait(bar, parity);
+            if (p.err) atomicOr(p.err, 1);
         }
-#pragma unroll
-        for (int q = 0; q < kRounds; ++q) {
-            const int idx = tid + q * kThreads;
-            if (idx < kBox) {
-                const int r = idx / (UC / 4), c4 = idx - r * (UC / 4);
-                st4(sUx + r * UC + 4 * c4, add4(v[q][0], v[q][2]));   // Ux = Px + Sx (PS:302)
-                st4(sUz + r * UC + 4 * c4, add4(v[q][1], v[q][3]));
-            }
-        }
+        __syncthreads();
+        return false;
+    }
+    for (int idx = tid; idx < G::UR * (UC / 4); idx += kThreads) {
+        st4(sUx + 4 * idx, add4(ld4(sUx + 4 * idx), ld4(stS + 4 * idx)));                  // Ux = Px + Sx (PS:302)
+        st4(sUz + 4 * idx, add4(ld4(sUz + 4 * idx), ld4(stS + G::UR * UC + 4 * idx)));     // Uz = Pz + Sz
     }
     if (MODE == kRcv && f.inj) {
         __syncthreads();
@@ -845,22 +894,29 @@ __device__ __forceinline__ void step_tile(const StepArgs& p, const Geo& gm, cons
             }
         }
     }
+    return true;
 }
 
 template <int N, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
-    extern __shared__ float4 smem4[];
+__global__ void __launch_bounds__(kThreads, 2) k_step(const __grid_constant__ StepArgs p) {
+    extern __shared__ __align__(128) float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4);
     using G = TileGeo<N>;
     const ShotDesc& d = p.shots[blockIdx.y];
     if ((int)blockIdx.x >= (MODE == kRec ? d.rec_tiles_x : d.tiles_x) * p.tiles_z) return;   // beyond this shot's width
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
     const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     const Geo gm = geo_of(d);
     prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
     const ShotView sv = shot_view(p, blockIdx.y);
     const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
-    step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f);
+    __syncthreads();   // the mbarrier is initialised
+    step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f, &bar, 0u);
 }
 
 // The same step as a persistent launch with a dynamic work queue: a few
@@ -871,11 +927,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const StepArgs p) {
 // end of the launch.  Each CTA claims its next item while it works on the
 // current one and prefetches that tile's operands to L2 right after it has
 // its index.  The last CTA to finish resets the counters for the next
-// launch of the same mode (no memset per launch).  No waits: a CTA only
-// atomically increments the counter and reads its value.
+// launch of the same mode (no memset per launch).  The queue has no waits:
+// a CTA only atomically increments the counter and reads its value (the
+// tile's own copy wait is bounded, as in k_step).
 template <int N, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) k_step_q(const StepArgs p, int nshots, int ntiles) {
-    extern __shared__ float4 smem4[];
+__global__ void __launch_bounds__(kThreads, 2) k_step_q(const __grid_constant__ StepArgs p, int nshots, int ntiles) {
+    extern __shared__ __align__(128) float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4);
     __shared__ int s_item[2];
     using G = TileGeo<N>;
@@ -883,9 +940,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_q(const StepArgs p, int ns
     int* done = counter + 1;
     const int* order = p.order[MODE == kRec ? 1 : 0];
     const int nitems = ntiles * nshots;
-    if (threadIdx.x == 0) s_item[0] = atomicAdd(counter, 1);
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        s_item[0] = atomicAdd(counter, 1);
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     int item = s_item[0], buf = 0;
+    unsigned parity = 0;   // phase of the mbarrier that the next tile's copies complete
     while (item < nitems) {
         if (threadIdx.x == 0) s_item[buf ^ 1] = atomicAdd(counter, 1);
         const int b = item % nshots, k = item / nshots;
@@ -897,7 +960,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_q(const StepArgs p, int ns
             prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
             const ShotView sv = shot_view(p, b);
             const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
-            step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f);
+            if (!step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f, &bar, parity)) break;   // uniform: reported
+            parity ^= 1u;
         }
         __syncthreads();   // the tile's shared memory is free and the next index is visible
         item = s_item[buf ^ 1];

@@ -82,13 +82,74 @@ static int launch_mode(Mode m, const StepArgs& a, int tiles_x, int nshots, cudaS
     return 1;
 }
 
+// Refuses (returns 1) a launch whose state map is missing or whose now[]
+// pointers are not fields of the mapped block, so that no step kernel runs
+// a tensor copy with coordinates the map does not describe.
 int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s) {
+    if (!a.state0 || a.fstride == 0 || a.nfields <= 0) return 1;
+    StepArgs b = a;
+    const float* f0 = a.state0 + (size_t)kGX * a.pitch + kZOFF;   // field 0 of slot 0, cell (0, 0)
+    for (int q = 0; q < 4; ++q) {
+        if (a.now[q] < f0) return 1;
+        const size_t d = (size_t)(a.now[q] - f0);
+        if (d % a.fstride != 0 || d / a.fstride >= (size_t)a.nfields) return 1;
+        b.now_field[q] = (int)(d / a.fstride);
+    }
     switch (N) {
-        case 2: return launch_mode<2>(mode, a, tiles_x, nshots, s);
-        case 5: return launch_mode<5>(mode, a, tiles_x, nshots, s);
-        case 6: return launch_mode<6>(mode, a, tiles_x, nshots, s);
+        case 2: return launch_mode<2>(mode, b, tiles_x, nshots, s);
+        case 5: return launch_mode<5>(mode, b, tiles_x, nshots, s);
+        case 6: return launch_mode<6>(mode, b, tiles_x, nshots, s);
     }
     return 1;
+}
+
+namespace {
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encoder() {
+    static EncodeTiled fn = []() -> EncodeTiled {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+
+template <int N>
+cudaError_t encode_for(StepArgs& a, const float* state0, int pitch, int rows, int nfields, int nslots, size_t fstride) {
+    using G = TileGeo<N>;
+    EncodeTiled enc = encoder();
+    if (!enc) return cudaErrorNotSupported;
+    // dimensions innermost first: columns, rows, fields, slots; strides in bytes
+    const cuuint64_t dims[4] = {(cuuint64_t)pitch, (cuuint64_t)rows, (cuuint64_t)nfields, (cuuint64_t)nslots};
+    const cuuint64_t strides[3] = {(cuuint64_t)pitch * 4, (cuuint64_t)fstride * 4, (cuuint64_t)fstride * nfields * 4};
+    const cuuint32_t box[4] = {(cuuint32_t)G::UC, (cuuint32_t)G::UR, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    static_assert((G::UC * 4) % 16 == 0, "the box's rows are whole 16-byte units");
+    if (reinterpret_cast<uintptr_t>(state0) % 16 != 0 || (pitch * 4) % 16 != 0 || (fstride * 4) % 16 != 0)
+        return cudaErrorInvalidValue;
+    const CUresult r = enc(&a.box_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(state0), dims, strides,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    a.state0 = state0;
+    a.fstride = fstride;
+    a.nfields = nfields;
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t encode_box_map(StepArgs& a, const float* state0, int pitch, int rows, int nfields, int nslots,
+                           size_t fstride, int N) {
+    a.state0 = nullptr;
+    if (N == 2) return encode_for<2>(a, state0, pitch, rows, nfields, nslots, fstride);
+    if (N == 5) return encode_for<5>(a, state0, pitch, rows, nfields, nslots, fstride);
+    if (N == 6) return encode_for<6>(a, state0, pitch, rows, nfields, nslots, fstride);
+    return cudaErrorInvalidValue;
 }
 
 int step_smem_bytes(int N) {

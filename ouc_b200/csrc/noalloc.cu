@@ -24,7 +24,10 @@
 //     contents: every call clears what must start at zero, and calls whose
 //     work overlaps on the GPU (different streams, or different host
 //     threads) race on it -- serialise them;
-//   * problems that do not fit the array are rejected with OUC_ESCRATCH.
+//   * problems that do not fit the array are rejected with OUC_ESCRATCH;
+//   * the step kernels' copy waits are bounded; the call itself returns
+//     before they run, so a wait that gives up (no such case is known) is
+//     reported in the output: both gathers are filled with NaN.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -84,6 +87,17 @@ __global__ void k_model(const ModelArgs m) {
 // copies (no host-to-device copy from pageable memory).
 __global__ void k_put_desc(ShotDesc* dst, const ShotDesc desc) { *dst = desc; }
 
+// After the run: if a step kernel recorded a failed copy wait, mark the
+// caller's gathers as invalid (NaN) -- the only report an asynchronous call
+// can give.
+__global__ void k_mark_failed(const int* status, float* gx, float* gz, size_t n) {
+    if (!(*status & 1)) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        gx[i] = __int_as_float(0x7fc00000);
+        gz[i] = __int_as_float(0x7fc00000);
+    }
+}
+
 }  // namespace
 
 extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, const float* d_vp,
@@ -139,14 +153,17 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     const size_t nfields = 4 + 24;   // model: vp2 vs2 ax az; state: now 4, past 4, F 2x4, O 8
     const size_t gather_floats = 2 * (size_t)nt * X;
     const size_t desc_at = (nfields * fstride + gather_floats + 63) / 64 * 64;   // 256-byte aligned
-    const size_t need = desc_at + (sizeof(ShotDesc) + 3) / 4;
+    const size_t status_at = desc_at + (sizeof(ShotDesc) + 3) / 4;   // one int: the kernels' status word
+    const size_t need = status_at + 1;
     if (need > kScratchFloats) return OUC_ESCRATCH;
     auto field = [&](size_t k) { return base + k * fstride + (size_t)kGX * pitch + kZOFF; };
     float* gathers = base + nfields * fstride;
     ShotDesc* d_desc = reinterpret_cast<ShotDesc*>(base + desc_at);
+    int* d_status = reinterpret_cast<int*>(base + status_at);
 
     // clear everything this call reads before writing (previous calls' contents)
     if (cudaMemsetAsync(base, 0, nfields * fstride * sizeof(float), stream) != cudaSuccess) return OUC_ECUDA;
+    if (cudaMemsetAsync(d_status, 0, sizeof(int), stream) != cudaSuccess) return OUC_ECUDA;
 
     ModelArgs m;
     memset(&m, 0, sizeof(m));
@@ -170,6 +187,7 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     desc.rec_tiles_x = tiles_x;
     desc.ring = Ring::make(X, Z, L, N);
     desc.off = 0;
+    desc.slot = 0;
     desc.strip_slot = 0;
     desc.vp2 = field(0); desc.vs2 = field(1); desc.ax = field(2); desc.az = field(3);
     desc.bx = nullptr; desc.bz = nullptr;   // density-normalised equations only
@@ -186,7 +204,11 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     a.shot_stride = 0;
     a.ring = Ring::make(X, Z, L, N);
     a.shots = d_desc;
+    a.err = d_status;
     a.record = 1;
+    // the tensor map of the scratch state block (its four leapfrog fields
+    // start at field 4); encoded on the host, passed with the arguments
+    if (encode_box_map(a, base, pitch, Xc + 2 * kGX, (int)nfields, 1, fstride, N) != cudaSuccess) return OUC_ECUDA;
     a.save = 0;
     float *now[4], *past[4], *fo[4], *fn[4], *o[8];
     size_t k = 4;
@@ -217,5 +239,6 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
                             stream) != cudaSuccess)
             return OUC_ECUDA;
     }
+    k_mark_failed<<<148, 256, 0, stream>>>(d_status, d_gather_vx, d_gather_vz, (size_t)nt * X);
     return cudaGetLastError() == cudaSuccess ? OUC_OK : OUC_ECUDA;
 }

@@ -12,6 +12,7 @@
 // Field pointers passed to kernels point at cell (0, 0): element (i, j) is
 // f[i * pitch + j] for i in [-GX, Xc+GX) and j in [-ZOFF, Zc+ZOFF).
 #pragma once
+#include <cuda.h>            // CUtensorMap (the type; its encoder is reached through the runtime)
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -135,6 +136,7 @@ struct ShotDesc {
     int rec_tiles_x;               // tile rows of the reconstruction (interior)
     Ring ring;                     // boundary ring of this grid
     size_t off;                    // offset (floats) of this shot's fields from shot 0's
+    int slot;                      // its index in the state block (off = slot * shot_stride)
     size_t strip_slot;             // floats per strip slot
     const float* vp2;              // model views of this grid, cell (0, 0): the moduli
     const float* vs2;              // (rho) Vp^2 and (rho) Vs^2, damping x and z,
@@ -145,6 +147,18 @@ struct ShotDesc {
 };
 
 struct StepArgs {
+    // 4-D tensor map of the state block (columns of the pitch, rows with the
+    // guard rows, field, shot slot) whose box is one tile's U box (UC x UR
+    // of TileGeo<N>): the step kernels bring the U box into shared memory
+    // with one cp.async.bulk.tensor per field.  state0 is the block's start
+    // (field 0 of slot 0, guard row and column 0); launch_step refuses a
+    // launch whose map is missing or whose now[] fields are not fields of
+    // the block, and fills now_field from now[].
+    alignas(64) CUtensorMap box_map;
+    const float* state0;
+    size_t fstride;                   // floats per field of the block
+    int nfields;                      // fields per shot slot of the block
+    int now_field[4];                 // field index of now[0..3]
     int X, Z, pitch, L;
     int tiles_z, tile_x0, tile_z0;    // tile columns of this launch; cell origin of its first tile
     int t;                            // time step index
@@ -250,6 +264,10 @@ struct GradStackArgs {
 };
 
 // Host-side launchers (kernels.cu)
+// Encode StepArgs::box_map for a state block at `state0` (nslots shot slots
+// of nfields fields of rows x pitch floats each) and half-order N.
+cudaError_t encode_box_map(StepArgs& a, const float* state0, int pitch, int rows, int nfields, int nslots,
+                           size_t fstride, int N);
 int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cudaStream_t s);
 // Segments of the x-marching kernel for a launch (rows of the widest shot).
 int march_segments(Mode mode, const StepArgs& a);
