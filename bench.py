@@ -105,12 +105,16 @@ def measured_peak():
 
 
 def committed_traffic():
-    p = os.path.join(ROOT, "profiles", "k_step_fwd_traffic.json")
+    """DRAM bytes per launch of the step kernels from the committed ncu
+    capture (profiles/k_step_traffic_c2_b16.json: a list of entries with
+    kernel, workload, batch, dram_bytes_per_launch), or []."""
+    p = os.path.join(ROOT, "profiles", "k_step_traffic_c2_b16.json")
     try:
         with open(p) as f:
-            return json.load(f)
+            d = json.load(f)
+        return d if isinstance(d, list) else [d]
     except Exception:
-        return None
+        return []
 
 
 def cpu_sample(steps_hint=None, threads=None, budget_s=12.0):
@@ -450,7 +454,10 @@ def main():
         for k, name in enumerate(("forward", "receiver", "reconstruction")):
             a_gbs = alg[name] / (iso[k] / 1e3) / 1e9
             kern[name] = {"kernel": kname(name), "launch_ms": iso[k], "algorithmic_bytes_per_launch": alg[name],
-                          "achieved": a_gbs, "frac": a_gbs / peak}
+                          "achieved": a_gbs, "frac": a_gbs / peak,
+                          "traffic": next((t.get("dram_bytes_per_launch") for t in committed_traffic()
+                                           if t.get("workload") == w.name and t.get("batch") == B and
+                                           t.get("kernel") == kname(name)), None)}
     per_launch_ms = statistics.median(fwd_ms) / nt        # forward launch, over the timed region
     dom = max(kern, key=lambda k: kern[k]["launch_ms"]) if kern else "forward"
     if dom == "forward":
@@ -458,9 +465,8 @@ def main():
     else:
         r_ms, r_bytes, r_src = kern[dom]["launch_ms"], alg[dom], "isolated launches (ouc_time_step_kernels)"
     achieved = r_bytes / (r_ms / 1e3) / 1e9
-    tr = committed_traffic()
-    traffic = tr.get("dram_bytes_per_launch") if tr and tr.get("workload") == w.name and tr.get("batch") == B and \
-        tr.get("kernel") == kname(dom) else None
+    traffic = next((t.get("dram_bytes_per_launch") for t in committed_traffic()
+                    if t.get("workload") == w.name and t.get("batch") == B and t.get("kernel") == kname(dom)), None)
 
     # saved source wavefield per shot: 8 ring fields per step (strip form) or
     # the two P components of every K-th imaging level (snapshot form)

@@ -320,6 +320,15 @@ int ouc_tune(ouc_ctx* ctx, int steps, int* best_batch, int* best_seg_rows, float
 int ouc_set_step_kernel(ouc_ctx* ctx, int seg_rows);
 int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows);
 
+/* Test hook for the step kernels' bounded copy wait (no counterpart in the
+ * reference).  on = 1: every tile of the tile kernels expects 16 bytes more
+ * than its tensor copies deliver, so each CTA's wait on them runs out (about
+ * 40 ms), records the failure and leaves its tile unwritten; the next
+ * whole-shot call returns OUC_ETIMEOUT and clears the record.  on = 0 (the
+ * default) restores normal operation; the context stays usable.  Drops the
+ * captured time loops. */
+int ouc_debug_copy_stall(ouc_ctx* ctx, int on);
+
 /* Device time of one launch of each step kernel at batch n (ms[0] forward,
  * ms[1] receiver, ms[2] reconstruction + imaging), averaged over `reps`
  * launches after one warm-up, on the state the last RTM batch of n shots

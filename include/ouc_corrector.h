@@ -27,8 +27,9 @@
  * zero), so a region at rest receives no correction.
  * Convolutions run as implicit GEMMs on the tensor cores (tcgen05, BF16
  * operands, FP32 accumulation in tensor memory); the input-gradient pass is
- * the same kernel on the flipped, transposed weights; weight gradients
- * accumulate in FP32.
+ * the same kernel on the flipped, transposed weights; weight gradients are
+ * tensor-core GEMMs over the pixels (BF16 operands, FP32 accumulation),
+ * reduced across CTAs in a fixed order, so training is reproducible.
  *
  * Parameters (FP32 master copy, ouc_cnn_nparams() floats): for each layer l
  * in order, W_l[cout][cin][5][5] (kx, kz: x-major as the grids) then b_l[cout].

@@ -55,6 +55,7 @@ SIGNATURES = {
     "ouc_set_step_kernel": (C.c_int, [_vp, C.c_int]),
     "ouc_tune": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "ouc_get_step_kernel": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "ouc_debug_copy_stall": (C.c_int, [_vp, C.c_int]),
     "ouc_time_step_kernels": (C.c_int, [_vp, C.c_int, C.c_int, _fp]),
     "ouc_stream": (_vp, [_vp]),
     "ouc_last_timing": (C.c_int, [_vp, C.POINTER(ouc_timing)]),

@@ -381,6 +381,11 @@ class Context:
         check(lib().ouc_time_step_kernels(self._h, int(n), int(reps), _p(ms)), self._h)
         return [float(x) for x in ms]
 
+    def debug_copy_stall(self, on):
+        """Test hook (ouc_debug_copy_stall): make the tile kernels' bounded
+        copy waits run out, so that the next call reports OUC_ETIMEOUT."""
+        check(lib().ouc_debug_copy_stall(self._h, int(bool(on))), self._h)
+
     def step_kernel(self):
         v = C.c_int()
         check(lib().ouc_get_step_kernel(self._h, C.byref(v)), self._h)

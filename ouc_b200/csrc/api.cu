@@ -171,6 +171,7 @@ StepArgs base_args(const ouc_ctx* c) {
     a.state0 = c->box_state0;
     a.fstride = c->fstride;
     a.nfields = kFieldsPerShot;
+    a.copy_tx_extra = c->copy_stall ? 16u : 0u;
     return a;
 }
 
@@ -947,6 +948,16 @@ int ouc_time_step_kernels(ouc_ctx* ctx, int n, int reps, float* ms) {
         ms[kind] = elapsed(ctx->ev[0], ctx->ev[1]) / reps;
     }
     return check_status(ctx);
+}
+
+int ouc_debug_copy_stall(ouc_ctx* ctx, int on) {
+    if (!ctx || (on != 0 && on != 1)) return OUC_EINVAL;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+    ctx->graphs.clear();
+    ctx->copy_stall = on != 0;
+    return OUC_OK;
 }
 
 int ouc_get_step_kernel(const ouc_ctx* ctx, int* seg_rows) {

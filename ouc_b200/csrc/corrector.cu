@@ -45,7 +45,7 @@ constexpr int kTile = 128;            // GEMM M: pixels per tile
 constexpr int kPC = kTile + 4;        // patch columns (2 + 2 halo)
 constexpr int kTaps = 25;
 constexpr int kMaxPairs = 32 * 32;     // (cin, cout) pairs of the widest layer
-constexpr int kMaxRowBlocks = 64;      // row blocks of k_wgrad
+constexpr int kMaxRowBlocks = 64;      // CTAs (partial-sum slots) of k_wgrad_tc
 constexpr int kBgradBlocks = 256;      // blocks of k_bgrad (8 warps each)
 constexpr int kThreadsConv = 128;
 
@@ -313,59 +313,178 @@ cudaError_t launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
     return cudaSuccess;
 }
 
-// ---- weight gradients (FP32), bias gradients, packing, Adam ---------------
-
-// dW[co][ci][tap] += sum_p X[p shifted by tap][ci] * G[p][co].  grid.x = tap,
-// grid.y = row blocks; each thread owns up to 4 (ci, co) pairs.
+// ---- weight gradients on the tensor cores ------------------------------------
+//
+// dW[tap][co][ci] = sum_p X[p + s(tap)][ci] G[p][co] over all pixels p, with
+// s(dx, dz) = (dx - 2, dz - 2).  The pixels are the GEMM's K dimension, so
+// the operand that carries the tap shift must move along K by whole 16-byte
+// rows: both operands use the no-swizzle MN-major layout, in which K
+// advances 16 bytes per pixel.  Per 128-pixel tile (one image row, as in
+// k_conv5) the CTA stages
+//   * the input patch, rows h-2..h+2 (plus zero rows up to 8) and columns
+//     z0-2..z0+129, as [row][channel chunk of 8][column][8 channels] -- the
+//     layout of k_conv5 -- so that M = 128 consecutive 8-channel groups are
+//     (row, chunk) pairs at one uniform stride: 4 rows x 32 channels (or 8 x
+//     16), and the tap shift dz is a start offset of 16 dz bytes;
+//   * the output gradient of the tile, [chunk of 8 output channels][pixel]
+//     [8 channels], the N operand;
+// and one thread issues, for each dz and row group, 8 MMAs of K = 16
+// (kind::f16, BF16 inputs, FP32 accumulation in tensor memory): D[(dx, ci)]
+// [co] for the tile's pixels, accumulated over all of the CTA's tiles.  At
+// the end each warp reads its 32 accumulator lanes (rows (dx, ci)) and
+// writes the CTA's partial sums, which k_wgrad_sum adds in CTA order: the
+// result does not depend on scheduling, so training repeats bit for bit.
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(256) k_wgrad(int n, int H, int W, const bf16* x, const bf16* g, int cin_real,
-                                               int cout_real, float* part) {
-    constexpr int PX = 32;
-    __shared__ float xs[PX][CIN + 1];
-    __shared__ float gs[PX][COUT + 1];
-    const int tap = blockIdx.x, dx = tap / 5 - 2, dz = tap % 5 - 2;
-    const int npairs = cin_real * cout_real;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    const int rows = n * H;
-    for (int row = blockIdx.y; row < rows; row += gridDim.y) {
-        const int img = row / H, h = row - img * H, sh = h + dx;
-        for (int z0 = 0; z0 < W; z0 += PX) {
-            __syncthreads();
-            for (int i = threadIdx.x; i < PX * CIN; i += 256) {
-                const int p = i / CIN, c = i % CIN, z = z0 + p, sz = z + dz;
-                float v = 0.f;
-                if (z < W && sh >= 0 && sh < H && sz >= 0 && sz < W)
-                    v = __bfloat162float(x[(((size_t)img * H + sh) * W + sz) * CIN + c]);
-                xs[p][c] = v;
-            }
-            for (int i = threadIdx.x; i < PX * COUT; i += 256) {
-                const int p = i / COUT, c = i % COUT, z = z0 + p;
-                gs[p][c] = z < W ? __bfloat162float(g[(((size_t)img * H + h) * W + z) * COUT + c]) : 0.f;
-            }
-            __syncthreads();
+struct WgradGeo {
+    static constexpr int NQ = CIN / 8;                  // input-channel chunks
+    static constexpr int RPG = 128 / CIN;               // patch rows per M = 128 row group
+    static constexpr int NRG = (5 + RPG - 1) / RPG;     // row groups covering dx = 0..4
+    static constexpr int PR = NRG * RPG;                // patch rows held (rows >= 5 stay zero)
+    static constexpr int p_bytes = PR * NQ * kPC * 16;
+    static constexpr int g_bytes = (COUT / 8) * kTile * 16;
+    static constexpr int bytes = p_bytes + g_bytes;
+    static constexpr int ncols = 5 * NRG * COUT;        // accumulator columns
+    static constexpr int tmem_cols = ncols <= 32 ? 32 : ncols <= 64 ? 64 : ncols <= 128 ? 128 : ncols <= 256 ? 256 : 512;
+    static_assert(ncols <= 512, "accumulators fit tensor memory");
+};
+
+// Instruction descriptor as idesc_bf16 with both operands MN-major
+// (bit 15: A, bit 16: B).
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) { return idesc_bf16(M, N) | (1u << 15) | (1u << 16); }
+
+// No-swizzle MN-major descriptor: 8 K rows of 16 bytes per core matrix, K
+// groups of 8 rows at `kgroup` bytes, M/N groups of 8 elements at `mgroup`
+// bytes (leading-dimension offset = K-group stride, stride offset = M/N
+// group stride for this layout).
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr, uint32_t kgroup, uint32_t mgroup) {
+    return umma_desc(saddr, kgroup, mgroup);
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreadsConv) k_wgrad_tc(int n, int H, int W, const bf16* x, const bf16* g,
+                                                        int cin_real, int cout_real, float* part, int* err) {
+    using G = WgradGeo<CIN, COUT>;
+    constexpr int NQ = G::NQ, NRG = G::NRG, PR = G::PR, QO = COUT / 8;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* s_p = smem;
+    uint8_t* s_g = smem + G::p_bytes;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // patch rows 5 .. PR-1 are read by the last row group's MMAs and stay zero
+    for (int i = tid; i < (PR - 5) * NQ * kPC; i += kThreadsConv)
+        reinterpret_cast<uint4*>(s_p + 5 * NQ * kPC * 16)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncwarp();
+    if (warp == 0) tmem_alloc(&tmem_base, G::tmem_cols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const int tiles_w = (W + kTile - 1) / kTile;
+    const int ntiles = n * H * tiles_w;
+    uint32_t phase = 0, acc = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int tw = tile % tiles_w, row = tile / tiles_w;
+        const int img = row / H, h = row - img * H;
+        const int z0 = tw * kTile;
+        for (int i = tid; i < 5 * kPC * NQ; i += kThreadsConv) {
+            const int q = i % NQ, rest = i / NQ, c = rest % kPC, r = rest / kPC;
+            const int gh = h + r - 2, gz = z0 + c - 2;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (gh >= 0 && gh < H && gz >= 0 && gz < W)
+                v = *reinterpret_cast<const uint4*>(x + (((size_t)img * H + gh) * W + gz) * CIN + q * 8);
+            *reinterpret_cast<uint4*>(s_p + ((size_t)(r * NQ + q) * kPC + c) * 16) = v;
+        }
+        for (int i = tid; i < kTile * QO; i += kThreadsConv) {
+            const int q = i % QO, c = i / QO, gz = z0 + c;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);   // pixels beyond the row add nothing
+            if (gz < W) v = *reinterpret_cast<const uint4*>(g + (((size_t)img * H + h) * W + gz) * COUT + q * 8);
+            *reinterpret_cast<uint4*>(s_g + ((size_t)q * kTile + c) * 16) = v;
+        }
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            const uint32_t pb = smem_u32(s_p), gb = smem_u32(s_g);
+            constexpr uint32_t idesc = idesc_bf16_mn(128, COUT);
+#pragma unroll 1
+            for (int dz = 0; dz < 5; ++dz) {
+#pragma unroll 1
+                for (int rg = 0; rg < NRG; ++rg) {
+                    const uint32_t d = tmem + (uint32_t)((dz * NRG + rg) * COUT);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int pr = threadIdx.x + 256 * k;
-                if (pr < npairs) {
-                    const int ci = pr % cin_real, co = pr / cin_real;
-                    float s = acc[k];
-#pragma unroll 8
-                    for (int p = 0; p < PX; ++p) s = fmaf(xs[p][ci], gs[p][co], s);
-                    acc[k] = s;
+                    for (int ks = 0; ks < kTile / 16; ++ks) {
+                        const uint64_t ad = umma_desc_mn(pb + ((rg * G::RPG * NQ) * kPC + dz + 16 * ks) * 16, 128,
+                                                         kPC * 16);
+                        const uint64_t bd = umma_desc_mn(gb + (16 * ks) * 16, 128, kTile * 16);
+                        umma_bf16(d, ad, bd, idesc, (acc | (uint32_t)ks) ? 1u : 0u);
+                    }
+                }
+            }
+            umma_commit(&bar);
+        }
+        acc = 1;
+        const bool done = mbar_wait(&bar, phase);
+        phase ^= 1u;
+        if (!__syncthreads_and(done)) {
+            if (tid == 0) atomicExch(err, 1);
+            mbar_wait(&bar, phase ^ 1u);   // one more bounded wait for the MMAs in flight
+            ok = false;
+            break;
+        }
+    }
+    tc_fence_after();
+    // accumulator row m = 32 warp + lane: 8-channel group j = m / 8 = (row in
+    // group, chunk), channel e = m % 8; column (dz, rg) * COUT + co
+    if (ok) {
+        const int m = warp * 32 + lane, j = m >> 3, e = m & 7;
+        const int ci = (j % NQ) * 8 + e;
+#pragma unroll 1
+        for (int dz = 0; dz < 5; ++dz) {
+#pragma unroll 1
+            for (int rg = 0; rg < NRG; ++rg) {
+                uint32_t r[COUT];
+                __syncwarp();
+                tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((dz * NRG + rg) * COUT), r);
+                const int dx = rg * G::RPG + j / NQ;
+                if (dx < 5 && ci < cin_real) {
+                    const int tap = dx * 5 + dz;
+                    float* out = part + ((size_t)blockIdx.x * kTaps + tap) * kMaxPairs;
+#pragma unroll
+                    for (int co = 0; co < COUT; ++co)
+                        if (co < cout_real) out[co * cin_real + ci] = __uint_as_float(r[co]);
                 }
             }
         }
     }
-    // this row block's partial sums, reduced in a fixed order by k_wgrad_sum
-    // (no atomics: training is reproducible run to run)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int pr = threadIdx.x + 256 * k;
-        if (pr < npairs) part[((size_t)blockIdx.y * kTaps + tap) * kMaxPairs + pr] = acc[k];
-    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    __syncwarp();
+    if (warp == 0) tmem_dealloc(tmem, G::tmem_cols);
 }
 
-// dw[co][ci][tap] += sum over the row blocks, in block order.
+template <int CIN, int COUT>
+cudaError_t launch_wgrad(int n, int H, int W, const bf16* x, const bf16* g, int cin_real, int cout_real, float* part,
+                         int* err, int* nblocks, cudaStream_t s) {
+    constexpr int bytes = WgradGeo<CIN, COUT>::bytes;
+    const cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    const int tiles = n * H * ((W + kTile - 1) / kTile);
+    // a fixed grid (at most kMaxRowBlocks partial-sum slots), independent of the device
+    const int grid = tiles < kMaxRowBlocks ? tiles : kMaxRowBlocks;
+    k_wgrad_tc<CIN, COUT><<<grid, kThreadsConv, bytes, s>>>(n, H, W, x, g, cin_real, cout_real, part, err);
+    *nblocks = grid;
+    return cudaSuccess;
+}
+
+// ---- gradient sums, bias gradients, packing, Adam ---------------------------
+
+// dw[co][ci][tap] += sum over the CTAs' partial sums, in CTA order.
 __global__ void k_wgrad_sum(int nblocks, int cin_real, int cout_real, const float* part, float* dw) {
     const int npairs = cin_real * cout_real;
     for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < kTaps * npairs; i += blockDim.x * gridDim.x) {
@@ -626,13 +745,14 @@ int ouc_cnn_backward_dev(ouc_cnn* net, const float* d_gout, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     const int n = net->n, H = net->H, W = net->W;
     const size_t P = (size_t)n * H * W;
-    const int rows = n * H;
-    const dim3 wg(kTaps, rows < kMaxRowBlocks ? rows : kMaxRowBlocks);
+    int nb = 0;   // CTAs of the weight-gradient launch: partial-sum slots to add
     k_to_bf16<<<1024, 256, 0, s>>>(P, OUC_CNN_OUT, 16, d_gout, net->g16);
     // layer 4: weights and bias, then the gradient into layer 3's output
     float* gp = net->grads;
-    k_wgrad<32, 16><<<wg, 256, 0, s>>>(n, H, W, net->y[2], net->g16, kL[3].cin, kL[3].cout, net->part);
-    k_wgrad_sum<<<64, 256, 0, s>>>(wg.y, kL[3].cin, kL[3].cout, net->part, gp + p_offset(3));
+    if (launch_wgrad<32, 16>(n, H, W, net->y[2], net->g16, kL[3].cin, kL[3].cout, net->part, net->err, &nb, s) !=
+        cudaSuccess)
+        return OUC_ECUDA;
+    k_wgrad_sum<<<64, 256, 0, s>>>(nb, kL[3].cin, kL[3].cout, net->part, gp + p_offset(3));
     k_bgrad<16><<<kBgradBlocks, 256, 0, s>>>(P, net->g16, kL[3].cout, net->part);
     k_bgrad_sum<<<1, 32, 0, s>>>(kBgradBlocks * 8, kL[3].cout, net->part, gp + p_offset(3) + w_count(3));
     ConvArgs a{};
@@ -642,8 +762,10 @@ int ouc_cnn_backward_dev(ouc_cnn* net, const float* d_gout, void* stream) {
     // layers 3 and 2
     for (int l = 2; l >= 1; --l) {
         const bf16* gl = net->g[(2 - l) & 1];
-        k_wgrad<32, 32><<<wg, 256, 0, s>>>(n, H, W, net->y[l - 1], gl, kL[l].cin, kL[l].cout, net->part);
-        k_wgrad_sum<<<64, 256, 0, s>>>(wg.y, kL[l].cin, kL[l].cout, net->part, gp + p_offset(l));
+        if (launch_wgrad<32, 32>(n, H, W, net->y[l - 1], gl, kL[l].cin, kL[l].cout, net->part, net->err, &nb, s) !=
+            cudaSuccess)
+            return OUC_ECUDA;
+        k_wgrad_sum<<<64, 256, 0, s>>>(nb, kL[l].cin, kL[l].cout, net->part, gp + p_offset(l));
         k_bgrad<32><<<kBgradBlocks, 256, 0, s>>>(P, gl, kL[l].cout, net->part);
         k_bgrad_sum<<<1, 32, 0, s>>>(kBgradBlocks * 8, kL[l].cout, net->part, gp + p_offset(l) + w_count(l));
         a.x = gl; a.w = net->wd[l]; a.mask = net->y[l - 1]; a.y = net->g[(3 - l) & 1];
@@ -651,8 +773,9 @@ int ouc_cnn_backward_dev(ouc_cnn* net, const float* d_gout, void* stream) {
     }
     // layer 1
     const bf16* g1 = net->g[0];
-    k_wgrad<16, 32><<<wg, 256, 0, s>>>(n, H, W, net->x0, g1, kL[0].cin, kL[0].cout, net->part);
-    k_wgrad_sum<<<64, 256, 0, s>>>(wg.y, kL[0].cin, kL[0].cout, net->part, gp + p_offset(0));
+    if (launch_wgrad<16, 32>(n, H, W, net->x0, g1, kL[0].cin, kL[0].cout, net->part, net->err, &nb, s) != cudaSuccess)
+        return OUC_ECUDA;
+    k_wgrad_sum<<<64, 256, 0, s>>>(nb, kL[0].cin, kL[0].cout, net->part, gp + p_offset(0));
     k_bgrad<32><<<kBgradBlocks, 256, 0, s>>>(P, g1, kL[0].cout, net->part);
     k_bgrad_sum<<<1, 32, 0, s>>>(kBgradBlocks * 8, kL[0].cout, net->part, gp + p_offset(0) + w_count(0));
     return cudaGetLastError() == cudaSuccess ? OUC_OK : OUC_ECUDA;

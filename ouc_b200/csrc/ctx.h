@@ -40,6 +40,7 @@ struct ouc_ctx {
     int batch = 1;               // shots the device state holds (cfg.max_batch)
     int run_batch = 1;           // shots advanced per launch (<= batch; ouc_tune_batch)
     int seg_rows = 0;            // step kernel: x-marching segments of this many rows, or 0 for 32 x 64 tiles
+    bool copy_stall = false;     // test hook (ouc_debug_copy_stall): tile copy waits run out
     int* d_status = nullptr;     // device status word: bit 0 a copy wait timed out, bit 1 a non-finite field
     int nsm = 148;               // SMs of the device
     int* d_queue = nullptr;      // dynamic-queue form: [mode][claim counter, finished CTAs]

@@ -502,7 +502,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                   "tensor-copy destinations are 128-byte aligned");
     const int err_word = p.err ? *(volatile const int*)p.err : 0;   // consumed after the wait
     if (tid == 0) {
-        mbar_arrive_tx(bar, 4u * G::UR * UC * 4u);
+        mbar_arrive_tx(bar, 4u * G::UR * UC * 4u + p.copy_tx_extra);
         // the previous tile's shared-memory accesses (generic proxy) precede these writes
         fence_proxy_async();
         // allocation coordinates: column ux_j0 + kZOFF (a multiple of 4), row ux_i0 + kGX (>= 0)

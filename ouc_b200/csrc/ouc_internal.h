@@ -159,6 +159,7 @@ struct StepArgs {
     size_t fstride;                   // floats per field of the block
     int nfields;                      // fields per shot slot of the block
     int now_field[4];                 // field index of now[0..3]
+    unsigned copy_tx_extra;           // test hook: bytes expected beyond the copies (0; ouc_debug_copy_stall)
     int X, Z, pitch, L;
     int tiles_z, tile_x0, tile_z0;    // tile columns of this launch; cell origin of its first tile
     int t;                            // time step index

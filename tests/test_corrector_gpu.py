@@ -1,5 +1,6 @@
 """The corrector network's tensor-core kernels (tcgen05 implicit-GEMM 5x5
-convolutions, forward and input-gradient passes; FP32 weight gradients)
+convolutions, forward and input-gradient passes, and tensor-core weight
+gradients)
 against the CPU restatement oracle/cnn.py, which rounds the same operands
 to bfloat16: outputs within 2e-3 and parameter gradients within 2e-2
 relative L2 per layer (the GPU accumulates in FP32 in another order, and an
