@@ -168,6 +168,7 @@ StepArgs base_args(const ouc_ctx* c) {
     a.ring = c->ring;
     a.shots = c->d_desc;
     a.box_map = c->box_map;
+    a.own_map = c->own_map;
     a.state0 = c->box_state0;
     a.fstride = c->fstride;
     a.nfields = kFieldsPerShot;
@@ -282,7 +283,6 @@ int upload_desc(ouc_ctx* ctx, int n, const ouc_shot* shots, const float* d_wavel
         d[b].rec_tiles_x = ctx->rec_tiles_x;
         d[b].ring = ctx->ring;
         d[b].off = (size_t)b * ctx->shot_stride;
-        d[b].slot = b;
         d[b].strip_slot = ctx->strip_slot;
         d[b].vp2 = ctx->vp2; d[b].vs2 = ctx->vs2; d[b].ax = ctx->ax; d[b].az = ctx->az;
         d[b].bx = ctx->bx; d[b].bz = ctx->bz;
@@ -865,6 +865,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
             cudaSuccess)
             return bad("cannot encode the state block's tensor map", OUC_ECUDA);
         ctx->box_map = m.box_map;
+        ctx->own_map = m.own_map;
         ctx->box_state0 = m.state0;
     }
     // kernel attributes set before any graph capture

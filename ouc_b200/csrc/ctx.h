@@ -47,6 +47,7 @@ struct ouc_ctx {
     int* d_order[2] = {nullptr, nullptr};   // its tile orders, heaviest first: full grid, reconstruction
     size_t fstride = 0;          // floats per field allocation
     alignas(64) CUtensorMap box_map;   // tensor map of the state block (StepArgs::box_map)
+    alignas(64) CUtensorMap own_map;   // and its own-cell box form (StepArgs::own_map)
     const float* box_state0 = nullptr;  // its start (null until encoded)
     size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;

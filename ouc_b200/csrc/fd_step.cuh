@@ -233,6 +233,14 @@ __device__ __forceinline__ void tma_box4(void* dst, const CUtensorMap* map, int 
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(b))
         : "memory");
 }
+// L2 prefetch of one box of a 4-D tensor map (no shared-memory write, no
+// completion to wait for).  Same coordinate rule as tma_box4.
+__device__ __forceinline__ void tma_prefetch_box4(const CUtensorMap* map, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Per-launch, per-shot constants.
@@ -422,30 +430,30 @@ __device__ __forceinline__ bool u_live(const StepArgs& p, const Geo& gm, int gi,
     return gi >= N && gi < gm.X - N && gj >= N && gj < p.Z - N;
 }
 
-// L2 prefetch of a tile's thread-loaded operands, one 128-byte line per
-// instruction, so that the loads of phases 2 and 3 find their lines in
-// flight or resident: the oldest level (read and overwritten in phase 3)
-// and, for the reconstruction, the receiver level and the imaging
-// accumulators over the own cells, and the model over the S region
-// (phase 2).  (The U box of phase 1 arrives by tensor copies.)  Every
-// address lies inside the field allocations (guard rows and columns
-// included).
+// L2 prefetch of a tile's thread-loaded operands, so that the loads of
+// phases 2 and 3 find their lines in flight or resident: the oldest level
+// (read and overwritten in phase 3) and, for the reconstruction, the
+// receiver level and the imaging accumulators over the own cells -- one
+// tensor prefetch per field (the state block's own-cell map) -- and the
+// model over the S region (phase 2), one 128-byte line per instruction
+// (every address inside the field allocations, guard rows and columns
+// included).  The U box of phase 1 arrives by tensor copies.
 template <int N, int MODE>
-__device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, size_t off, int x0, int z0) {
+__device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, int x0, int z0, int slot) {
     using G = TileGeo<N>;
     constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS;
     const int tid = threadIdx.x;
     const int P = p.pitch;
-    // own rows: TZ / 32 + 1 lines, as the tile need not start on a line
-    constexpr int kOwnPer = TZ / 32 + 1;
-    constexpr int kOwnLines = TX * kOwnPer;
-    for (int k = tid; k < 4 * kOwnLines; k += kThreads) {
-        const int f = k / kOwnLines, l = k - f * kOwnLines;
-        const int g = (x0 + l / kOwnPer) * P + z0 + 32 * (l % kOwnPer);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(p.past[f] + off + g));
-        if (MODE == kRec) {
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(p.rcv[f] + off + g));
-            if (f < 3) asm volatile("prefetch.global.L2 [%0];" ::"l"(p.acc[f] + off + g));
+    // own cells of the oldest level (and, reconstructing, of the receiver
+    // level and the accumulators): one tensor prefetch per field
+    if (tid == 32) {
+        const int c0 = z0 + kZOFF, c1 = x0 + kGX;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            if (p.past_field[f] >= 0) tma_prefetch_box4(&p.own_map, c0, c1, p.past_field[f], slot);
+            if (MODE == kRec && p.rcv_field[f] >= 0) tma_prefetch_box4(&p.own_map, c0, c1, p.rcv_field[f], slot);
+            if (MODE == kRec && f < 3 && p.acc_field[f] >= 0)
+                tma_prefetch_box4(&p.own_map, c0, c1, p.acc_field[f], slot);
         }
     }
     constexpr int kSPer = (TZ + 2 * HS + 31) / 32 + 1;
@@ -457,12 +465,39 @@ __device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, 
     }
 }
 
+// Issue the four tensor copies of a tile's U box (one thread): the UC x UR
+// box of each P/S field of the current level, completing on the CTA's
+// mbarrier -- P into the U arrays, S into the S-stage area, which is unused
+// until phase 2.  The whole 83 KB box is in flight at once and no thread
+// holds it in registers.  Called as early as the tile is known, so that the
+// copies overlap the tile's set-up.  `slot` is the shot's index in the
+// launch, which is its slot in the state block (its fields lie slot x
+// shot_stride floats after shot 0's).
+template <int N>
+__device__ __forceinline__ void issue_u_box(const StepArgs& p, float* sm, int x0, int z0, int slot, uint64_t* bar) {
+    using G = TileGeo<N>;
+    static_assert(G::floats - G::oTh >= 2 * G::UR * G::UC, "S staging fits the S-stage area");
+    static_assert((G::oUz * 4) % 128 == 0 && (G::oTh * 4) % 128 == 0 && (G::UR * G::UC * 4) % 128 == 0,
+                  "tensor-copy destinations are 128-byte aligned");
+    mbar_arrive_tx(bar, 4u * G::UR * G::UC * 4u + p.copy_tx_extra);
+    // a previous tile's shared-memory accesses (generic proxy) precede these writes
+    fence_proxy_async();
+    // allocation coordinates: column z0 - HU + kZOFF (a multiple of 4), row x0 - SHX - N + kGX (>= 0)
+    const int c0 = z0 - G::HU + kZOFF, c1 = x0 - G::SHX - N + kGX;
+    float* stS = sm + G::oTh;
+    tma_box4(sm + G::oUx, &p.box_map, c0, c1, p.now_field[0], slot, bar);
+    tma_box4(sm + G::oUz, &p.box_map, c0, c1, p.now_field[1], slot, bar);
+    tma_box4(stS, &p.box_map, c0, c1, p.now_field[2], slot, bar);
+    tma_box4(stS + G::UR * G::UC, &p.box_map, c0, c1, p.now_field[3], slot, bar);
+}
+
 // Offsets within one field are 32-bit ints (row * pitch + column, guard rows
 // negative): ouc_create refuses grids whose field allocation exceeds 2^31
 // floats, and the 32-bit multiply-adds are fewer instructions than the
 // 64-bit ones (+1.3 % measured).
-// One tile's step.  `bar` is the CTA's mbarrier (initialised, count 1) and
-// `parity` the phase that this tile's copies complete.  Returns false, with
+// One tile's step, after issue_u_box.  `bar` is the CTA's mbarrier
+// (initialised, count 1) and `parity` the phase that this tile's copies
+// complete.  Returns false, with
 // bit 0 of *p.err set, when the copies did not land within the wait's bound
 // (or an earlier launch had recorded such a failure): the tile is then left
 // unwritten and the host reports OUC_ETIMEOUT after the call.
@@ -491,27 +526,10 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
     const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;   // global origin of the U box
 
     // ---- phase 1: U = P + S over the tile and a 2N halo ---------------------
-    // One thread issues four tensor copies (cp.async.bulk.tensor, the UC x
-    // UR box of each P/S field of the current level, completing on the CTA's
-    // mbarrier): P into the U arrays, S into the S-stage area, which is
-    // unused until phase 2.  The whole 83 KB box is in flight at once and no
-    // thread holds it in registers.  One shared-memory pass then adds S to P.
+    // The box's four tensor copies were issued at the start of the tile
+    // (issue_u_box); wait for them, then one shared-memory pass adds S to P.
     float* stS = sm + G::oTh;   // Sx then Sz staging, UR x UC each
-    static_assert(G::floats - G::oTh >= 2 * G::UR * UC, "S staging fits the S-stage area");
-    static_assert((G::oUz * 4) % 128 == 0 && (G::oTh * 4) % 128 == 0 && (G::UR * UC * 4) % 128 == 0,
-                  "tensor-copy destinations are 128-byte aligned");
     const int err_word = p.err ? *(volatile const int*)p.err : 0;   // consumed after the wait
-    if (tid == 0) {
-        mbar_arrive_tx(bar, 4u * G::UR * UC * 4u + p.copy_tx_extra);
-        // the previous tile's shared-memory accesses (generic proxy) precede these writes
-        fence_proxy_async();
-        // allocation coordinates: column ux_j0 + kZOFF (a multiple of 4), row ux_i0 + kGX (>= 0)
-        const int c0 = ux_j0 + kZOFF, c1 = ux_i0 + kGX, slot = p.shots[sv.b].slot;
-        tma_box4(sUx, &p.box_map, c0, c1, p.now_field[0], slot, bar);
-        tma_box4(sUz, &p.box_map, c0, c1, p.now_field[1], slot, bar);
-        tma_box4(stS, &p.box_map, c0, c1, p.now_field[2], slot, bar);
-        tma_box4(stS + G::UR * UC, &p.box_map, c0, c1, p.now_field[3], slot, bar);
-    }
     const bool landed = mbar_wait(bar, parity);
     if (!__syncthreads_and(landed && !(err_word & 1))) {
         // a failed wait: one more bounded wait lets copies in flight land
@@ -902,17 +920,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const __grid_constant__ St
     extern __shared__ __align__(128) float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4);
     using G = TileGeo<N>;
-    const ShotDesc& d = p.shots[blockIdx.y];
-    if ((int)blockIdx.x >= (MODE == kRec ? d.rec_tiles_x : d.tiles_x) * p.tiles_z) return;   // beyond this shot's width
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
     const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
     __shared__ uint64_t bar;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {   // the tile's copies first: they overlap everything up to phase 1
         mbar_init(&bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue_u_box<N>(p, sm, x0, z0, blockIdx.y, &bar);
+    }
+    const ShotDesc& d = p.shots[blockIdx.y];
+    if ((int)blockIdx.x >= (MODE == kRec ? d.rec_tiles_x : d.tiles_x) * p.tiles_z) {
+        // beyond this shot's width (per-shot sub-grids): the copies (of cells
+        // outside the shot's grid) land before the shared memory is released
+        if (threadIdx.x == 0) mbar_wait(&bar, 0u);
+        return;
     }
     const Geo gm = geo_of(d);
-    prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
+    prefetch_tile<N, MODE>(p, gm, x0, z0, blockIdx.y);
     const ShotView sv = shot_view(p, blockIdx.y);
     const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
     __syncthreads();   // the mbarrier is initialised
@@ -956,8 +980,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_q(const __grid_constant__ 
         const ShotDesc& d = p.shots[b];
         if (tx < (MODE == kRec ? d.rec_tiles_x : d.tiles_x)) {   // within this shot's width
             const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
+            if (threadIdx.x == 0) issue_u_box<N>(p, sm, x0, z0, b, &bar);
             const Geo gm = geo_of(d);
-            prefetch_tile<N, MODE>(p, gm, d.off, x0, z0);
+            prefetch_tile<N, MODE>(p, gm, x0, z0, b);
             const ShotView sv = shot_view(p, b);
             const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
             if (!step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f, &bar, parity)) break;   // uniform: reported

@@ -89,11 +89,17 @@ int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cu
     if (!a.state0 || a.fstride == 0 || a.nfields <= 0) return 1;
     StepArgs b = a;
     const float* f0 = a.state0 + (size_t)kGX * a.pitch + kZOFF;   // field 0 of slot 0, cell (0, 0)
+    auto field_of = [&](const float* q) -> int {
+        if (!q || q < f0) return -1;
+        const size_t d = (size_t)(q - f0);
+        return d % a.fstride == 0 && d / a.fstride < (size_t)a.nfields ? (int)(d / a.fstride) : -1;
+    };
     for (int q = 0; q < 4; ++q) {
-        if (a.now[q] < f0) return 1;
-        const size_t d = (size_t)(a.now[q] - f0);
-        if (d % a.fstride != 0 || d / a.fstride >= (size_t)a.nfields) return 1;
-        b.now_field[q] = (int)(d / a.fstride);
+        b.now_field[q] = field_of(a.now[q]);
+        if (b.now_field[q] < 0) return 1;
+        b.past_field[q] = field_of(a.past[q]);
+        b.rcv_field[q] = field_of(a.rcv[q]);
+        if (q < 3) b.acc_field[q] = field_of(a.acc[q]);
     }
     switch (N) {
         case 2: return launch_mode<2>(mode, b, tiles_x, nshots, s);
@@ -136,6 +142,11 @@ cudaError_t encode_for(StepArgs& a, const float* state0, int pitch, int rows, in
                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const cuuint32_t own[4] = {(cuuint32_t)G::TZ, (cuuint32_t)G::TX, 1, 1};
+    const CUresult r2 = enc(&a.own_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(state0), dims, strides,
+                            own, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r2 != CUDA_SUCCESS) return cudaErrorInvalidValue;
     a.state0 = state0;
     a.fstride = fstride;
     a.nfields = nfields;

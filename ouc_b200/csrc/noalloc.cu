@@ -187,7 +187,6 @@ extern "C" int ouc_forward_noalloc(const ouc_config* cfg, const ouc_shot* shot, 
     desc.rec_tiles_x = tiles_x;
     desc.ring = Ring::make(X, Z, L, N);
     desc.off = 0;
-    desc.slot = 0;
     desc.strip_slot = 0;
     desc.vp2 = field(0); desc.vs2 = field(1); desc.ax = field(2); desc.az = field(3);
     desc.bx = nullptr; desc.bz = nullptr;   // density-normalised equations only

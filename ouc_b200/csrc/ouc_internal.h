@@ -135,8 +135,8 @@ struct ShotDesc {
     int tiles_x;                   // tile rows of the full step
     int rec_tiles_x;               // tile rows of the reconstruction (interior)
     Ring ring;                     // boundary ring of this grid
-    size_t off;                    // offset (floats) of this shot's fields from shot 0's
-    int slot;                      // its index in the state block (off = slot * shot_stride)
+    size_t off;                    // offset (floats) of this shot's fields from shot 0's: b * shot_stride
+                                   // for shot b of a launch (the tensor copies address slot b)
     size_t strip_slot;             // floats per strip slot
     const float* vp2;              // model views of this grid, cell (0, 0): the moduli
     const float* vs2;              // (rho) Vp^2 and (rho) Vs^2, damping x and z,
@@ -155,10 +155,12 @@ struct StepArgs {
     // launch whose map is missing or whose now[] fields are not fields of
     // the block, and fills now_field from now[].
     alignas(64) CUtensorMap box_map;
+    alignas(64) CUtensorMap own_map;     // the same block, box = one tile's own cells (TZ x TX): L2 prefetches
     const float* state0;
     size_t fstride;                   // floats per field of the block
     int nfields;                      // fields per shot slot of the block
     int now_field[4];                 // field index of now[0..3]
+    int past_field[4], rcv_field[4], acc_field[3];   // field indices of past, rcv, acc (-1: not in the block)
     unsigned copy_tx_extra;           // test hook: bytes expected beyond the copies (0; ouc_debug_copy_stall)
     int X, Z, pitch, L;
     int tiles_z, tile_x0, tile_z0;    // tile columns of this launch; cell origin of its first tile

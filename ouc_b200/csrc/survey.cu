@@ -120,7 +120,6 @@ int upload_batch(ouc_ctx* ctx, int n, const ouc_shot* shots, const ouc_aperture*
         s.rec_tiles_x = rec_tiles_for(w.X, L);
         s.ring = Ring::make(w.X, Z, L, ctx->N);
         s.off = (size_t)b * ctx->shot_stride;
-        s.slot = b;
         s.strip_slot = ctx->strip_slot;
         s.vp2 = slot_field(ctx, b, 0); s.vs2 = slot_field(ctx, b, 1);
         s.ax = slot_field(ctx, b, 2); s.az = slot_field(ctx, b, 3);
