@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_march(const StepArgs p) {
     float a[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) a[k] = p.a[k];
-    const Div dvx{p.dx, p.rdx}, dvz{p.dz, p.rdz};
+    const Div dvx = make_div(p.dx, p.rdx), dvz = make_div(p.dz, p.rdz);
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);

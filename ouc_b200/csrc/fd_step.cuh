@@ -105,23 +105,36 @@ __device__ __forceinline__ float4 mul4s(float4 a, float s) { return cat4(mul2(lo
 __device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
 struct Div {
-    float h, r;   // spacing and RN(1/h)
+    float h, r;    // spacing and RN(1/h)
+    unsigned tb;   // 2 bits(T) - 1: dividends with 0 < |x| < T take the double-precision path
 };
+// T bounds every dividend whose quotient estimate RN(x r) lies below 2^-124:
+// such an x has |x| < 2^-124 / r <= 2^-124 h (1 + 2^-23) (r = RN(1/h)), so
+// T = 2^-124 h (1 + 2^-22), each product rounded up.
+__device__ __forceinline__ Div make_div(float h, float r) {
+    const float t = __fmul_ru(__fmul_ru(h, 1.0f + 0x1p-22f), 0x1p-124f);
+    return Div{h, r, __float_as_uint(t) * 2u - 1u};
+}
 
 // Quotients below 2^-124 (the subnormal neighbourhood, common ahead of a
 // wavefront) are divided in double precision and rounded once more to float:
 // with 53 >= 2*24 + 2 bits the double rounding is innocuous (S. Figueroa,
 // "When is double rounding innocuous?", SIGNUM Newsletter 30(3), 1995), and
-// it avoids the slow subnormal path of single-precision division.  The guarded
-// form equals IEEE single division for every float dividend in
-// [2^-149, 2^-99) and the normal binades checked (exhaustive test on sm_100a).
-__device__ __forceinline__ bool tiny_q(float q0, float x) { return fabsf(q0) < 0x1p-124f && x != 0.f; }
+// it avoids the slow subnormal path of single-precision division.  The guard
+// tests the dividend (0 < |x| < T, Div::tb), a superset of the dividends
+// whose quotient estimate lies below 2^-124; the double path is exact for all
+// of them.  The guarded form equals IEEE single division for every float
+// dividend in [2^-149, 2^-99) and the normal binades checked (exhaustive test
+// on sm_100a).
 __device__ __forceinline__ float ddiv_f(float x, float h) { return __double2float_rn(__ddiv_rn((double)x, (double)h)); }
 __device__ __forceinline__ float4 div4(float4 x, const Div& d) {
     const float2 q0l = mul2(lo2(x), dup2(d.r)), q0h = mul2(hi2(x), dup2(d.r));
     float4 q = cat4(fma2(fma2(q0l, dup2(-d.h), lo2(x)), dup2(d.r), q0l),
                     fma2(fma2(q0h, dup2(-d.h), hi2(x)), dup2(d.r), q0h));
-    if (tiny_q(q0l.x, x.x) || tiny_q(q0l.y, x.y) || tiny_q(q0h.x, x.z) || tiny_q(q0h.y, x.w))
+    // 0 < |x| < T, on the bits: 2 bits(x) - 1 drops the sign and wraps a zero to the largest value
+    const bool tiny = (__float_as_uint(x.x) * 2u - 1u < d.tb) | (__float_as_uint(x.y) * 2u - 1u < d.tb) |
+                      (__float_as_uint(x.z) * 2u - 1u < d.tb) | (__float_as_uint(x.w) * 2u - 1u < d.tb);
+    if (tiny)
         q = make_float4(ddiv_f(x.x, d.h), ddiv_f(x.y, d.h), ddiv_f(x.z, d.h), ddiv_f(x.w, d.h));
     return q;
 }
@@ -520,7 +533,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
     float a[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) a[k] = p.a[k];
-    const Div dvx{p.dx, p.rdx}, dvz{p.dz, p.rdz};
+    const Div dvx = make_div(p.dx, p.rdx), dvz = make_div(p.dz, p.rdz);
     const size_t off = sv.off;
     const float* nowp[4] = {p.now[0] + off, p.now[1] + off, p.now[2] + off, p.now[3] + off};
     const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;   // global origin of the U box

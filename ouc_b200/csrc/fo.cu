@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_fo(const FoArgs p) {
     float a[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) a[k] = p.a[k];
-    const Div dvx{p.dx, p.rdx}, dvz{p.dz, p.rdz};
+    const Div dvx = make_div(p.dx, p.rdx), dvz = make_div(p.dz, p.rdz);
     const float dt = p.dt;
     const int ux_i0 = x0 - SHX - N, ux_j0 = z0 - HU;
 
