@@ -935,6 +935,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const __grid_constant__ St
     using G = TileGeo<N>;
     const int tz = blockIdx.x % p.tiles_z, tx = blockIdx.x / p.tiles_z;
     const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
+    if (MODE != kRec && x0 >= p.X - N) {
+        // every row of the tile lies outside the update domain [N, X-N) of
+        // the forward and receiver steps: its cells are never written (they
+        // were zeroed with the shot's state), so only the forward's record
+        // samples of these rows, zeros, are stored (PS:307-311 records every x)
+        if (MODE == kFwd && p.record) {
+            const ShotDesc& d = p.shots[blockIdx.y];
+            if (d.rz >= z0 && d.rz < z0 + G::TZ)
+                for (int i = x0 + (int)threadIdx.x; i < min(x0 + G::TX, d.X); i += kThreads) {
+                    d.gather_x[(size_t)p.t * d.X + i] = 0.f;
+                    d.gather_z[(size_t)p.t * d.X + i] = 0.f;
+                }
+        }
+        return;
+    }
     __shared__ uint64_t bar;
     if (threadIdx.x == 0) {   // the tile's copies first: they overlap everything up to phase 1
         mbar_init(&bar, 1);
