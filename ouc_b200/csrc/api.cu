@@ -169,6 +169,7 @@ StepArgs base_args(const ouc_ctx* c) {
     a.shots = c->d_desc;
     a.box_map = c->box_map;
     a.own_map = c->own_map;
+    a.s_map = c->s_map;
     a.state0 = c->box_state0;
     a.fstride = c->fstride;
     a.nfields = kFieldsPerShot;
@@ -866,6 +867,7 @@ int ouc_create(const ouc_config* cfg, const float* vp, const float* vs, const fl
             return bad("cannot encode the state block's tensor map", OUC_ECUDA);
         ctx->box_map = m.box_map;
         ctx->own_map = m.own_map;
+        ctx->s_map = m.s_map;
         ctx->box_state0 = m.state0;
     }
     // kernel attributes set before any graph capture

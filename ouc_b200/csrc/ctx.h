@@ -48,6 +48,7 @@ struct ouc_ctx {
     size_t fstride = 0;          // floats per field allocation
     alignas(64) CUtensorMap box_map;   // tensor map of the state block (StepArgs::box_map)
     alignas(64) CUtensorMap own_map;   // and its own-cell box form (StepArgs::own_map)
+    alignas(64) CUtensorMap s_map;     // and its S-region box form (StepArgs::s_map)
     const float* box_state0 = nullptr;  // its start (null until encoded)
     size_t shot_stride = 0;      // floats per shot block (kFieldsPerShot fields)
     int tiles_x = 0, tiles_z = 0;

@@ -419,8 +419,13 @@ __device__ __forceinline__ void for_ring(const Ring& R, int i0, int i1, int j0, 
         const int ia = max(i0, bi0), ib = min(i1, bi1), ja = max(j0, bj0), jb = min(j1, bj1);
         if (ia >= ib || ja >= jb) continue;
         const int w = jb - ja, n = (ib - ia) * w;
+        // k / w as a multiply-high by m = ceil(2^32 / w): exact for k < 2^16
+        // and w <= 2^16 (the error k (m - 2^32 / w) / 2^32 < 2^-16 stays
+        // below 1/w); the rectangles here hold well under 2^16 cells
+        const unsigned m = w > 1 ? 0xFFFFFFFFu / (unsigned)w + 1u : 0u;
         for (int k = threadIdx.x; k < n; k += kThreads) {
-            const int i = ia + k / w, j = ja + k % w;
+            const int q = w > 1 ? (int)__umulhi((unsigned)k, m) : k;
+            const int i = ia + q, j = ja + (k - q * w);
             f(i, j, base + (i - bi0) * stride + (j - bj0));
         }
     }
@@ -458,6 +463,46 @@ __device__ __forceinline__ TileFlags tile_flags(const StepArgs& p, const Geo& gm
     return f;
 }
 
+// L2 prefetch of the strip elements that a reconstruction tile restores:
+// the ring cells of its U box (slot_u: Ux, Uz) and of its S region (slot_s:
+// theta, omega and the four Q fields), over the same band rectangles as
+// for_ring.  The strips were written during the forward pass and come from
+// DRAM; prefetched at the tile's start, their latency runs under the U-box
+// copy and the S-stage instead of stalling the restore loops.  One 128-byte
+// line per prefetch, at element addresses inside the strip slots.
+template <int N>
+__device__ __forceinline__ void prefetch_ring(const StepArgs& p, const Geo& gm, const ShotDesc& d, int x0, int z0) {
+    using G = TileGeo<N>;
+    const Ring& R = gm.ring;
+    const int L = R.L, X = R.X, Z = R.Z, n2 = 2 * R.N, W = R.W, hm = R.H - 4 * R.N;
+    const int eb = strip_elem_bytes(p.strip_prec), per_line = 128 / eb;
+#pragma unroll 1
+    for (int part = 0; part < 2; ++part) {
+        const int i0 = part ? x0 - G::SHX : x0 - G::SHX - N, i1 = part ? x0 + G::TX + G::SHX : x0 - G::SHX - N + G::UR;
+        const int j0 = part ? z0 - G::HS : z0 - G::HU, j1 = part ? z0 + G::TZ + G::HS : z0 - G::HU + G::UC;
+        const char* slot = static_cast<const char*>(strip_slot_ptr(p, d, part ? p.slot_s : p.slot_u));
+        const int f0 = part ? (int)kSTh : (int)kSUx, nf = part ? 6 : 2;
+#pragma unroll 1
+        for (int b = 0; b < 4; ++b) {
+            int bi0, bi1, bj0, bj1, base, stride;
+            if (b == 0) { bi0 = L - R.N; bi1 = X - L + R.N; bj0 = L - R.N; bj1 = L + R.N; base = 0; stride = n2; }
+            else if (b == 1) { bi0 = L - R.N; bi1 = X - L + R.N; bj0 = Z - L - R.N; bj1 = Z - L + R.N; base = W * n2; stride = n2; }
+            else if (b == 2) { bi0 = L - R.N; bi1 = L + R.N; bj0 = L + R.N; bj1 = Z - L - R.N; base = 2 * W * n2; stride = hm; }
+            else { bi0 = X - L - R.N; bi1 = X - L + R.N; bj0 = L + R.N; bj1 = Z - L - R.N; base = 2 * W * n2 + n2 * hm; stride = hm; }
+            const int ia = max(i0, bi0), ib = min(i1, bi1), ja = max(j0, bj0), jb = min(j1, bj1);
+            if (ia >= ib || ja >= jb) continue;
+            const int rows = ib - ia, nl = (jb - ja + per_line - 1) / per_line;   // lines of one row's run
+            for (int k = threadIdx.x; k < nf * rows * nl; k += kThreads) {
+                const int f = k / (rows * nl), rem = k - f * (rows * nl);
+                const int row = rem / nl, l = rem - row * nl;
+                // element of the run: l * per_line < jb - ja
+                const int e = base + (ia + row - bi0) * stride + (ja - bj0) + l * per_line;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(slot + ((size_t)(f0 + f) * R.R + e) * eb));
+            }
+        }
+    }
+}
+
 template <int N, int MODE>
 __device__ __forceinline__ bool u_live(const StepArgs& p, const Geo& gm, int gi, int gj) {
     if (MODE == kRec) return gi >= p.L && gi < gm.X - p.L && gj >= p.L && gj < p.Z - p.L;
@@ -473,7 +518,8 @@ __device__ __forceinline__ bool u_live(const StepArgs& p, const Geo& gm, int gi,
 // (every address inside the field allocations, guard rows and columns
 // included).  The U box of phase 1 arrives by tensor copies.
 template <int N, int MODE>
-__device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, int x0, int z0, int slot) {
+__device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, int x0, int z0, int slot,
+                                              const TileFlags& fl) {
     using G = TileGeo<N>;
     constexpr int TX = G::TX, TZ = G::TZ, SHX = G::SHX, HS = G::HS;
     const int tid = threadIdx.x;
@@ -490,12 +536,32 @@ __device__ __forceinline__ void prefetch_tile(const StepArgs& p, const Geo& gm, 
                 tma_prefetch_box4(&p.own_map, c0, c1, p.acc_field[f], slot);
         }
     }
+    // in tiles that meet the damping layers: the S-stage CPML memories over
+    // the S region and the U-stage ones over the own cells, the fields that
+    // the tile's layers (x, z) use
+    if (MODE != kRec && tid == 64 && (fl.px || fl.pz)) {
+        const int s0 = z0 - HS + kZOFF, s1 = x0 - SHX + kGX, c0 = z0 + kZOFF, c1 = x0 + kGX;
+        // S-stage: x layers xx (0) and zx (3), z layers zz (1) and xz (2)
+#pragma unroll
+        for (int f = 0; f < 4; ++f)
+            if (((f == 0 || f == 3) ? fl.px : fl.pz) && p.fold_field[f] >= 0)
+                tma_prefetch_box4(&p.s_map, s0, s1, p.fold_field[f], slot);
+        // U-stage: z layers C A Tz Wz (0 3 5 6), x layers E B Tx Wx (1 2 4 7)
+#pragma unroll
+        for (int f = 0; f < 8; ++f)
+            if (((f == 0 || f == 3 || f == 5 || f == 6) ? fl.pz : fl.px) && p.o_field[f] >= 0)
+                tma_prefetch_box4(&p.own_map, c0, c1, p.o_field[f], slot);
+    }
+    // the model over the S region: Vp^2, Vs^2 and, in damping tiles, the
+    // damping profiles of the tile's layers
     constexpr int kSPer = (TZ + 2 * HS + 31) / 32 + 1;
     constexpr int kSLines = (TX + 2 * SHX) * kSPer;
-    for (int k = tid; k < 2 * kSLines; k += kThreads) {
+    const int nm = MODE == kRec ? 2 : 2 + (fl.px ? 1 : 0) + (fl.pz ? 1 : 0);
+    for (int k = tid; k < nm * kSLines; k += kThreads) {
         const int f = k / kSLines, l = k - f * kSLines;
         const int g = (x0 - SHX + l / kSPer) * P + (z0 - HS) + 32 * (l % kSPer);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"((f ? gm.vs2 : gm.vp2) + g));
+        const float* m = f == 0 ? gm.vp2 : f == 1 ? gm.vs2 : (f == 2 && fl.px) ? gm.ax : gm.az;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(m + g));
     }
 }
 
@@ -985,9 +1051,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(const __grid_constant__ St
         return;
     }
     const Geo gm = geo_of(d);
-    prefetch_tile<N, MODE>(p, gm, x0, z0, blockIdx.y);
     const ShotView sv = shot_view(p, blockIdx.y);
     const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
+    prefetch_tile<N, MODE>(p, gm, x0, z0, blockIdx.y, f);
+    if (MODE == kRec && f.ring) prefetch_ring<N>(p, gm, d, x0, z0);
     __syncthreads();   // the mbarrier is initialised
     step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f, &bar, 0u);
 }
@@ -1031,9 +1098,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_q(const __grid_constant__ 
             const int x0 = p.tile_x0 + tx * G::TX, z0 = p.tile_z0 + tz * G::TZ;
             if (threadIdx.x == 0) issue_u_box<N>(p, sm, x0, z0, b, &bar);
             const Geo gm = geo_of(d);
-            prefetch_tile<N, MODE>(p, gm, x0, z0, b);
             const ShotView sv = shot_view(p, b);
             const TileFlags f = tile_flags<N, MODE>(p, gm, sv, x0, z0);
+            prefetch_tile<N, MODE>(p, gm, x0, z0, b, f);
+            if (MODE == kRec && f.ring) prefetch_ring<N>(p, gm, d, x0, z0);
             if (!step_tile<N, MODE>(p, gm, sv, sm, x0, z0, f, &bar, parity)) break;   // uniform: reported
             parity ^= 1u;
         }

@@ -100,7 +100,9 @@ int launch_step(int N, Mode mode, const StepArgs& a, int tiles_x, int nshots, cu
         b.past_field[q] = field_of(a.past[q]);
         b.rcv_field[q] = field_of(a.rcv[q]);
         if (q < 3) b.acc_field[q] = field_of(a.acc[q]);
+        b.fold_field[q] = field_of(a.f_old[q]);
     }
+    for (int q = 0; q < 8; ++q) b.o_field[q] = field_of(a.o[q]);
     switch (N) {
         case 2: return launch_mode<2>(mode, b, tiles_x, nshots, s);
         case 5: return launch_mode<5>(mode, b, tiles_x, nshots, s);
@@ -147,6 +149,11 @@ cudaError_t encode_for(StepArgs& a, const float* state0, int pitch, int rows, in
                             own, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r2 != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const cuuint32_t sbox[4] = {(cuuint32_t)G::SC, (cuuint32_t)G::SR, 1, 1};
+    const CUresult r3 = enc(&a.s_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(state0), dims, strides,
+                            sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r3 != CUDA_SUCCESS) return cudaErrorInvalidValue;
     a.state0 = state0;
     a.fstride = fstride;
     a.nfields = nfields;

@@ -156,11 +156,13 @@ struct StepArgs {
     // the block, and fills now_field from now[].
     alignas(64) CUtensorMap box_map;
     alignas(64) CUtensorMap own_map;     // the same block, box = one tile's own cells (TZ x TX): L2 prefetches
+    alignas(64) CUtensorMap s_map;       // the same block, box = one tile's S region (SC x SR): L2 prefetches
     const float* state0;
     size_t fstride;                   // floats per field of the block
     int nfields;                      // fields per shot slot of the block
     int now_field[4];                 // field index of now[0..3]
     int past_field[4], rcv_field[4], acc_field[3];   // field indices of past, rcv, acc (-1: not in the block)
+    int o_field[8], fold_field[4];                   // and of the U- and S-stage CPML memories
     unsigned copy_tx_extra;           // test hook: bytes expected beyond the copies (0; ouc_debug_copy_stall)
     int X, Z, pitch, L;
     int tiles_z, tile_x0, tile_z0;    // tile columns of this launch; cell origin of its first tile
