@@ -492,9 +492,13 @@ __device__ __forceinline__ void prefetch_ring(const StepArgs& p, const Geo& gm, 
             const int ia = max(i0, bi0), ib = min(i1, bi1), ja = max(j0, bj0), jb = min(j1, bj1);
             if (ia >= ib || ja >= jb) continue;
             const int rows = ib - ia, nl = (jb - ja + per_line - 1) / per_line;   // lines of one row's run
-            for (int k = threadIdx.x; k < nf * rows * nl; k += kThreads) {
-                const int f = k / (rows * nl), rem = k - f * (rows * nl);
-                const int row = rem / nl, l = rem - row * nl;
+            // row-major (field, row, line) index decoded by multiply-high, as in for_ring
+            const int per_f = rows * nl;
+            const unsigned mf = per_f > 1 ? 0xFFFFFFFFu / (unsigned)per_f + 1u : 0u;
+            const unsigned ml = nl > 1 ? 0xFFFFFFFFu / (unsigned)nl + 1u : 0u;
+            for (int k = threadIdx.x; k < nf * per_f; k += kThreads) {
+                const int f = per_f > 1 ? (int)__umulhi((unsigned)k, mf) : k, rem = k - f * per_f;
+                const int row = nl > 1 ? (int)__umulhi((unsigned)rem, ml) : rem, l = rem - row * nl;
                 // element of the run: l * per_line < jb - ja
                 const int e = base + (ia + row - bi0) * stride + (ja - bj0) + l * per_line;
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(slot + ((size_t)(f0 + f) * R.R + e) * eb));
@@ -664,10 +668,15 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
         const ShotDesc& d = p.shots[sv.b];
         const void* su = strip_slot_ptr(p, d, p.slot_u);
         const unsigned* am = d.amax ? d.amax + (size_t)p.slot_u * kStripFields : nullptr;
+        // both loads before the stores: a shared store through a generic
+        // pointer would otherwise order the second load behind the first
+        // load's round trip
         for_ring(gm.ring, ux_i0, ux_i0 + G::UR, ux_j0, ux_j0 + UC, [&](int i, int j, int ri) {
             const int o = (i - ux_i0) * UC + (j - ux_j0);
-            sUx[o] = strip_get(p, su, am, kSUx, kSUx * R + ri);
-            sUz[o] = strip_get(p, su, am, kSUz, kSUz * R + ri);
+            const float ux = strip_get(p, su, am, kSUx, kSUx * R + ri);
+            const float uz = strip_get(p, su, am, kSUz, kSUz * R + ri);
+            sUx[o] = ux;
+            sUz[o] = uz;
         });
     }
     __syncthreads();
@@ -786,21 +795,35 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
             // read_wavefiled2 (PS:1377-1424): theta, omega and the Q fields of the ring
             const void* ss = strip_slot_ptr(p, d, p.slot_s);
             const unsigned* am = d.amax ? d.amax + (size_t)p.slot_s * kStripFields : nullptr;
+            // all six loads before any store (see the U restore above)
             for_ring(gm.ring, x0 - SHX, x0 + TX + SHX, z0 - HS, z0 + TZ + HS, [&](int i, int j, int ri) {
                 const int r = i - x0, c = j - z0;
                 const bool rin = r >= 0 && r < TX, cin = c >= 0 && c < TZ;
+                float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 if (rin || cin) {
-                    const int o = (r + SHX) * SC + (c + HS);
-                    sTh[o] = strip_get(p, ss, am, kSTh, kSTh * R + ri);
-                    sOm[o] = strip_get(p, ss, am, kSOm, kSOm * R + ri);
+                    v[0] = strip_get(p, ss, am, kSTh, kSTh * R + ri);
+                    v[1] = strip_get(p, ss, am, kSOm, kSOm * R + ri);
                 }
                 if (cin) {
-                    sQxz[(r + SHX) * TZ + c] = strip_get(p, ss, am, kSQxz, kSQxz * R + ri);
-                    sQzz[(r + SHX) * TZ + c] = strip_get(p, ss, am, kSQzz, kSQzz * R + ri);
+                    v[2] = strip_get(p, ss, am, kSQxz, kSQxz * R + ri);
+                    v[3] = strip_get(p, ss, am, kSQzz, kSQzz * R + ri);
                 }
                 if (rin) {
-                    sQxx[r * SC + (c + HS)] = strip_get(p, ss, am, kSQxx, kSQxx * R + ri);
-                    sQzx[r * SC + (c + HS)] = strip_get(p, ss, am, kSQzx, kSQzx * R + ri);
+                    v[4] = strip_get(p, ss, am, kSQxx, kSQxx * R + ri);
+                    v[5] = strip_get(p, ss, am, kSQzx, kSQzx * R + ri);
+                }
+                if (rin || cin) {
+                    const int o = (r + SHX) * SC + (c + HS);
+                    sTh[o] = v[0];
+                    sOm[o] = v[1];
+                }
+                if (cin) {
+                    sQxz[(r + SHX) * TZ + c] = v[2];
+                    sQzz[(r + SHX) * TZ + c] = v[3];
+                }
+                if (rin) {
+                    sQxx[r * SC + (c + HS)] = v[4];
+                    sQzx[r * SC + (c + HS)] = v[5];
                 }
             });
         }
@@ -1005,9 +1028,11 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
 #pragma unroll
                 for (int q = 0; q < kStripFields; ++q) k[q] = f16_exp(am[q]);
                 for_ring(gm.ring, x0, x0 + TX, z0, z0 + TZ, [&](int, int, int ri) {
+                    float v[kStripFields];   // all loads before the stores
 #pragma unroll
-                    for (int q = 0; q < kStripFields; ++q)
-                        dst[q * R + ri] = __float2half_rn(scale2(src[q * R + ri], k[q]));
+                    for (int q = 0; q < kStripFields; ++q) v[q] = src[q * R + ri];
+#pragma unroll
+                    for (int q = 0; q < kStripFields; ++q) dst[q * R + ri] = __float2half_rn(scale2(v[q], k[q]));
                 });
             }
         }
