@@ -49,6 +49,10 @@
 
 #include "ouc_internal.h"
 
+#ifndef P2DZ
+#define P2DZ 0
+#endif
+
 namespace ouc {
 
 template <int N>
@@ -102,6 +106,12 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) { return cat4(add2(lo
 __device__ __forceinline__ float4 sub4(float4 a, float4 b) { return cat4(sub2(lo2(a), lo2(b)), sub2(hi2(a), hi2(b))); }
 __device__ __forceinline__ float4 mul4(float4 a, float4 b) { return cat4(mul2(lo2(a), lo2(b)), mul2(hi2(a), hi2(b))); }
 __device__ __forceinline__ float4 mul4s(float4 a, float s) { return cat4(mul2(lo2(a), dup2(s)), mul2(hi2(a), dup2(s))); }
+// Field accesses of phases 2 and 3 in the global space (ld/st.global.cg,
+// cached in L2 only): unlike accesses through generic pointers, the
+// compiler may order them freely against the shared-memory accesses
+// (-1 to -3 % per launch measured).
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void stg4(float* p, float4 v) { __stcg(reinterpret_cast<float4*>(p), v); }
 __device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
 struct Div {
@@ -707,33 +717,47 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
 #pragma unroll
         for (int qq = 0; qq < P2R; ++qq) {
             const int g = (x0 + r0 + q0 + qq) * P + (z0 + c);
-            vp2r[qq] = ld4(gm.vp2 + g);
-            vs2r[qq] = ld4(gm.vs2 + g);
+            vp2r[qq] = ldg4(gm.vp2 + g);
+            vs2r[qq] = ldg4(gm.vs2 + g);
         }
         float4 exx[P2R], ezx[P2R];
         dx4<N, P2R, false>(ux0 + q0 * UC, UC, a, dvx, exx);   // dvxdx = D-x Ux
         dx4<N, P2R, true>(uz0 + q0 * UC, UC, a, dvx, ezx);    // dvzdx = D+x Uz
+#if P2DZ
+        // both rows' z-derivatives before the first row's shared-memory
+        // stores, which would otherwise order the second row's loads
+        float4 exzr[P2R], ezzr[P2R];
+#pragma unroll
+        for (int qq = 0; qq < P2R; ++qq) {
+            exzr[qq] = dz4<N, true>(ux0 + (q0 + qq) * UC, a, dvz);    // dvxdz = D+z Ux
+            ezzr[qq] = dz4<N, false>(uz0 + (q0 + qq) * UC, a, dvz);   // dvzdz = D-z Uz
+        }
+#endif
 #pragma unroll
         for (int qq = 0; qq < P2R; ++qq) {
             const int q = q0 + qq;
             const int r = r0 + q;
             const int gi = x0 + r;
             const int gjb = z0 + c;
+#if P2DZ
+            const float4 exz = exzr[qq], ezz = ezzr[qq];
+#else
             const float4 exz = dz4<N, true>(ux0 + q * UC, a, dvz);    // dvxdz = D+z Ux
             const float4 ezz = dz4<N, false>(uz0 + q * UC, a, dvz);   // dvzdz = D-z Uz
+#endif
             const int g = gi * P + gjb;
             const float4 vp2 = vp2r[qq], vs2 = vs2r[qq];
             const bool own = ownc && r >= 0 && r < TX;
             float4 fxx = zero4(), fzz = zero4(), fxz = zero4(), fzx = zero4();
             if (f.px) {
-                const float4 axv = ld4(gm.ax + g);
-                fxx = cpml4(ld4(p.f_old[0] + off + g), axv, exx[qq], p.dt);
-                fzx = cpml4(ld4(p.f_old[3] + off + g), axv, ezx[qq], p.dt);
+                const float4 axv = ldg4(gm.ax + g);
+                fxx = cpml4(ldg4(p.f_old[0] + off + g), axv, exx[qq], p.dt);
+                fzx = cpml4(ldg4(p.f_old[3] + off + g), axv, ezx[qq], p.dt);
             }
             if (f.pz) {
-                const float4 azv = ld4(gm.az + g);
-                fzz = cpml4(ld4(p.f_old[1] + off + g), azv, ezz, p.dt);
-                fxz = cpml4(ld4(p.f_old[2] + off + g), azv, exz, p.dt);
+                const float4 azv = ldg4(gm.az + g);
+                fzz = cpml4(ldg4(p.f_old[1] + off + g), azv, ezz, p.dt);
+                fxz = cpml4(ldg4(p.f_old[2] + off + g), azv, exz, p.dt);
             }
             // theta = Vp^2 (exx + ezz - Fxx - Fzz), omega = Vs^2 (exz - ezx - Fxz + Fzx) (PS:373-378);
             // outside the damping layers the memories are exact zeros and
@@ -759,8 +783,8 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                 }
             }
             if (own) {
-                if (f.px) { st4(p.f_new[0] + off + g, fxx); st4(p.f_new[3] + off + g, fzx); }
-                if (f.pz) { st4(p.f_new[1] + off + g, fzz); st4(p.f_new[2] + off + g, fxz); }
+                if (f.px) { stg4(p.f_new[0] + off + g, fxx); stg4(p.f_new[3] + off + g, fzx); }
+                if (f.pz) { stg4(p.f_new[1] + off + g, fzz); stg4(p.f_new[2] + off + g, fxz); }
             }
             const int sr = r + SHX, scol = c + HS;
             st4(sTh + sr * SC + scol, th);
@@ -861,10 +885,10 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
             const int gi = x0 + r;
             const int g = gi * P + (z0 + c);
             // the leapfrog's operands first: their latency runs under the derivatives
-            const float4 npx = ld4(nowp[0] + g), npz = ld4(nowp[1] + g);
-            const float4 nsx = ld4(nowp[2] + g), nsz = ld4(nowp[3] + g);
-            const float4 opx = ld4(p.past[0] + off + g), opz = ld4(p.past[1] + off + g);
-            const float4 osx = ld4(p.past[2] + off + g), osz = ld4(p.past[3] + off + g);
+            const float4 npx = ldg4(nowp[0] + g), npz = ldg4(nowp[1] + g);
+            const float4 nsx = ldg4(nowp[2] + g), nsz = ldg4(nowp[3] + g);
+            const float4 opx = ldg4(p.past[0] + off + g), opz = ldg4(p.past[1] + off + g);
+            const float4 osx = ldg4(p.past[2] + off + g), osz = ldg4(p.past[3] + off + g);
             float4 tx[1], wx[1], dB[1], dE[1];
             dx4<N, 1, true>(sTh + (r + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
             dx4<N, 1, false>(sOm + (r + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
@@ -877,18 +901,18 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
             float4 oC = zero4(), oE = zero4(), oB = zero4(), oA = zero4();
             float4 oTx = zero4(), oTz = zero4(), oWz = zero4(), oWx = zero4();
             if (f.pz) {
-                const float4 d = ld4(gm.az + g);
-                oC = cpml4(ld4(p.o[0] + off + g), d, dC, dt);
-                oA = cpml4(ld4(p.o[3] + off + g), d, dA, dt);
-                oTz = cpml4(ld4(p.o[5] + off + g), d, tz, dt);
-                oWz = cpml4(ld4(p.o[6] + off + g), d, wz, dt);
+                const float4 d = ldg4(gm.az + g);
+                oC = cpml4(ldg4(p.o[0] + off + g), d, dC, dt);
+                oA = cpml4(ldg4(p.o[3] + off + g), d, dA, dt);
+                oTz = cpml4(ldg4(p.o[5] + off + g), d, tz, dt);
+                oWz = cpml4(ldg4(p.o[6] + off + g), d, wz, dt);
             }
             if (f.px) {
-                const float4 d = ld4(gm.ax + g);
-                oE = cpml4(ld4(p.o[1] + off + g), d, dE[0], dt);
-                oB = cpml4(ld4(p.o[2] + off + g), d, dB[0], dt);
-                oTx = cpml4(ld4(p.o[4] + off + g), d, tx[0], dt);
-                oWx = cpml4(ld4(p.o[7] + off + g), d, wx[0], dt);
+                const float4 d = ldg4(gm.ax + g);
+                oE = cpml4(ldg4(p.o[1] + off + g), d, dE[0], dt);
+                oB = cpml4(ldg4(p.o[2] + off + g), d, dB[0], dt);
+                oTx = cpml4(ldg4(p.o[4] + off + g), d, tx[0], dt);
+                oWx = cpml4(ldg4(p.o[7] + off + g), d, wx[0], dt);
             }
             // leapfrog brackets in the reference's order (PS:291-294); zero
             // memories outside the damping layers change no rounding
@@ -898,7 +922,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
             float4 ssx = add4(sub4(sub4(add4(sub4(wz, oWz), dC), dE[0]), oC), oE);
             float4 ssz = add4(sub4(sub4(add4(add4(nwx, oWx), dB[0]), dA), oB), oA);
             if (p.density) {   // variable density: acceleration = buoyancy x stress divergence
-                const float4 bxv = ld4(gm.bx + g), bzv = ld4(gm.bz + g);
+                const float4 bxv = ldg4(gm.bx + g), bzv = ldg4(gm.bz + g);
                 spx = mul4(spx, bxv); ssx = mul4(ssx, bxv);
                 spz = mul4(spz, bzv); ssz = mul4(ssz, bzv);
             }
@@ -940,8 +964,8 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                 // zero-lag imaging condition (corr_v, PS:1426-1439) on the interior
                 const float4 sx = p.img_past ? opx : npx;
                 const float4 sz = p.img_past ? opz : npz;
-                const float4 rpx = ld4(p.rcv[0] + off + g), rpz = ld4(p.rcv[1] + off + g);
-                const float4 rsx = ld4(p.rcv[2] + off + g), rsz = ld4(p.rcv[3] + off + g);
+                const float4 rpx = ldg4(p.rcv[0] + off + g), rpz = ldg4(p.rcv[1] + off + g);
+                const float4 rsx = ldg4(p.rcv[2] + off + g), rsz = ldg4(p.rcv[3] + off + g);
                 float* acc0 = p.acc[0] + off + g;
                 float* acc1 = p.acc[1] + off + g;
                 float* acc2 = p.acc[2] + off + g;
@@ -949,7 +973,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                     return cat4(add2(lo2(acc), fma2(lo2(a1), lo2(b1), mul2(lo2(a2), lo2(b2)))),
                                 add2(hi2(acc), fma2(hi2(a1), hi2(b1), mul2(hi2(a2), hi2(b2)))));
                 };
-                const float4 o0 = ld4(acc0), o1 = ld4(acc1), o2 = ld4(acc2);
+                const float4 o0 = ldg4(acc0), o1 = ldg4(acc1), o2 = ldg4(acc2);
                 if (!p.comp_image) {
                     float4 npp = corr(o0, sx, rpx, sz, rpz);
                     float4 nil = corr(o2, sx, sx, sz, sz);
@@ -962,7 +986,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                             }
                         }
                     }
-                    st4(acc0, npp); st4(acc1, nps); st4(acc2, nil);
+                    stg4(acc0, npp); stg4(acc1, nps); stg4(acc2, nil);
                 } else {
                     // compensated sums (Kahan, CACM 8(1), 1965): acc + c carries the
                     // sum to about twice float precision; c holds minus the
@@ -975,7 +999,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                     float* accp[3] = {acc0, acc1, acc2};
 #pragma unroll
                     for (int q = 0; q < 3; ++q) {
-                        const float4 cq = ld4(cp[q]);
+                        const float4 cq = ldg4(cp[q]);
                         float4 na = old[q], nc = cq;
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
@@ -985,20 +1009,20 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
                             set_comp(nc, k, __fsub_rn(__fsub_rn(t, comp(old[q], k)), y));
                             set_comp(na, k, t);
                         }
-                        st4(accp[q], na);
-                        st4(cp[q], nc);
+                        stg4(accp[q], na);
+                        stg4(cp[q], nc);
                     }
                 }
             }
-            st4(p.past[0] + off + g, vpx); st4(p.past[1] + off + g, vpz);
-            st4(p.past[2] + off + g, vsx); st4(p.past[3] + off + g, vsz);
+            stg4(p.past[0] + off + g, vpx); stg4(p.past[1] + off + g, vpz);
+            stg4(p.past[2] + off + g, vsx); stg4(p.past[3] + off + g, vsz);
             if (f.pz) {
-                st4(p.o[0] + off + g, oC); st4(p.o[3] + off + g, oA);
-                st4(p.o[5] + off + g, oTz); st4(p.o[6] + off + g, oWz);
+                stg4(p.o[0] + off + g, oC); stg4(p.o[3] + off + g, oA);
+                stg4(p.o[5] + off + g, oTz); stg4(p.o[6] + off + g, oWz);
             }
             if (f.px) {
-                st4(p.o[1] + off + g, oE); st4(p.o[2] + off + g, oB);
-                st4(p.o[4] + off + g, oTx); st4(p.o[7] + off + g, oWx);
+                stg4(p.o[1] + off + g, oE); stg4(p.o[2] + off + g, oB);
+                stg4(p.o[4] + off + g, oTx); stg4(p.o[7] + off + g, oWx);
             }
         }
     }
