@@ -49,10 +49,6 @@
 
 #include "ouc_internal.h"
 
-#ifndef P2DZ
-#define P2DZ 0
-#endif
-
 namespace ouc {
 
 template <int N>
@@ -723,28 +719,14 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
         float4 exx[P2R], ezx[P2R];
         dx4<N, P2R, false>(ux0 + q0 * UC, UC, a, dvx, exx);   // dvxdx = D-x Ux
         dx4<N, P2R, true>(uz0 + q0 * UC, UC, a, dvx, ezx);    // dvzdx = D+x Uz
-#if P2DZ
-        // both rows' z-derivatives before the first row's shared-memory
-        // stores, which would otherwise order the second row's loads
-        float4 exzr[P2R], ezzr[P2R];
-#pragma unroll
-        for (int qq = 0; qq < P2R; ++qq) {
-            exzr[qq] = dz4<N, true>(ux0 + (q0 + qq) * UC, a, dvz);    // dvxdz = D+z Ux
-            ezzr[qq] = dz4<N, false>(uz0 + (q0 + qq) * UC, a, dvz);   // dvzdz = D-z Uz
-        }
-#endif
 #pragma unroll
         for (int qq = 0; qq < P2R; ++qq) {
             const int q = q0 + qq;
             const int r = r0 + q;
             const int gi = x0 + r;
             const int gjb = z0 + c;
-#if P2DZ
-            const float4 exz = exzr[qq], ezz = ezzr[qq];
-#else
             const float4 exz = dz4<N, true>(ux0 + q * UC, a, dvz);    // dvxdz = D+z Ux
             const float4 ezz = dz4<N, false>(uz0 + q * UC, a, dvz);   // dvzdz = D-z Uz
-#endif
             const int g = gi * P + gjb;
             const float4 vp2 = vp2r[qq], vs2 = vs2r[qq];
             const bool own = ownc && r >= 0 && r < TX;
