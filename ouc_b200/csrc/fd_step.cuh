@@ -859,6 +859,19 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
         const int c = 4 * (tid % (TZ / 4));
         const int scol = c + HS;
         const float dt = p.dt;
+        // receiver and reconstruction: the four x derivatives of both rows
+        // from one window pass (11 shared-memory loads per derivative instead
+        // of 20; measured 1.8-2.0 % faster at c2, batch 16).  The forward
+        // keeps one row per pass: the carried values cost it spills and the
+        // pass is no faster there.
+        constexpr bool kPairX = MODE != kFwd;
+        float4 txr[2], wxr[2], dBr[2], dEr[2];
+        if constexpr (kPairX) {
+            dx4<N, 2, true>(sTh + (rr + SHX) * SC + scol, SC, a, dvx, txr);    // dthetadx = D+x theta
+            dx4<N, 2, false>(sOm + (rr + SHX) * SC + scol, SC, a, dvx, wxr);   // domegadx = D-x omega
+            dx4<N, 2, false>(sQxz + (rr + SHX) * TZ + c, TZ, a, dvx, dBr);     // dux_zdx = D-x Qxz
+            dx4<N, 2, true>(sQzz + (rr + SHX) * TZ + c, TZ, a, dvx, dEr);      // duz_zdx = D+x Qzz
+        }
         // a rolled two-iteration loop: half the code of an unrolled pair of
         // rows, which keeps the hot path inside the instruction cache
 #pragma unroll 1
@@ -872,10 +885,15 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
             const float4 opx = ldg4(p.past[0] + off + g), opz = ldg4(p.past[1] + off + g);
             const float4 osx = ldg4(p.past[2] + off + g), osz = ldg4(p.past[3] + off + g);
             float4 tx[1], wx[1], dB[1], dE[1];
-            dx4<N, 1, true>(sTh + (r + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
-            dx4<N, 1, false>(sOm + (r + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
-            dx4<N, 1, false>(sQxz + (r + SHX) * TZ + c, TZ, a, dvx, dB);     // dux_zdx = D-x Qxz
-            dx4<N, 1, true>(sQzz + (r + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
+            if constexpr (kPairX) {
+                tx[0] = txr[0]; wx[0] = wxr[0]; dB[0] = dBr[0]; dE[0] = dEr[0];
+                txr[0] = txr[1]; wxr[0] = wxr[1]; dBr[0] = dBr[1]; dEr[0] = dEr[1];
+            } else {
+                dx4<N, 1, true>(sTh + (r + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
+                dx4<N, 1, false>(sOm + (r + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
+                dx4<N, 1, false>(sQxz + (r + SHX) * TZ + c, TZ, a, dvx, dB);     // dux_zdx = D-x Qxz
+                dx4<N, 1, true>(sQzz + (r + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
+            }
             const float4 tz = dz4<N, true>(sTh + (r + SHX) * SC + scol, a, dvz);    // dthetadz
             const float4 wz = dz4<N, false>(sOm + (r + SHX) * SC + scol, a, dvz);   // domegadz
             const float4 dA = dz4<N, true>(sQxx + r * SC + scol, a, dvz);           // dux_xdz = D+z Qxx
