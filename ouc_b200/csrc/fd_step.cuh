@@ -859,18 +859,42 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
         const int c = 4 * (tid % (TZ / 4));
         const int scol = c + HS;
         const float dt = p.dt;
-        // receiver and reconstruction: the four x derivatives of both rows
-        // from one window pass (11 shared-memory loads per derivative instead
-        // of 20; measured 1.8-2.0 % faster at c2, batch 16).  The forward
-        // keeps one row per pass: the carried values cost it spills and the
-        // pass is no faster there.
-        constexpr bool kPairX = MODE != kFwd;
+        // The x derivatives of a thread's two rows come from one window pass
+        // (11 shared-memory loads per derivative instead of 20).  Where the
+        // second row's values would stay in registers through the row loop
+        // they cost spills, so the U box, free once the S-stage has read it,
+        // holds them instead (one float4 per thread and value, stride
+        // kThreads, conflict-free):
+        //  - forward: tx, wx and dB of both rows above the first TX x TZ
+        //    floats of the two U fields (those keep the new U for the strip
+        //    pass); dE one row per pass;
+        //  - receiver: all four of both rows from the start of the U fields;
+        //  - reconstruction: the second row's values carried in registers;
+        //  - U boxes too small for the above (N = 2): one row per pass.
+        // Measured at c2, batch 16: forward -1.9 %, receiver -3.0 %,
+        // reconstruction -2.0 % against one row per pass.
+        constexpr bool kShare3 = MODE == kFwd && G::UR * G::UC >= TX * TZ + 12 * kThreads;
+        constexpr bool kShare4 = MODE == kRcv && G::UR * G::UC >= 16 * kThreads;
+        constexpr bool kCarry = MODE == kRec;
+        float4* const c3x = reinterpret_cast<float4*>(sUx + TX * TZ) + tid;
+        float4* const c3z = reinterpret_cast<float4*>(sUz + TX * TZ) + tid;
+        float4* const c4x = reinterpret_cast<float4*>(sUx) + tid;
+        float4* const c4z = reinterpret_cast<float4*>(sUz) + tid;
         float4 txr[2], wxr[2], dBr[2], dEr[2];
-        if constexpr (kPairX) {
+        if constexpr (kCarry || kShare3 || kShare4) {
             dx4<N, 2, true>(sTh + (rr + SHX) * SC + scol, SC, a, dvx, txr);    // dthetadx = D+x theta
             dx4<N, 2, false>(sOm + (rr + SHX) * SC + scol, SC, a, dvx, wxr);   // domegadx = D-x omega
             dx4<N, 2, false>(sQxz + (rr + SHX) * TZ + c, TZ, a, dvx, dBr);     // dux_zdx = D-x Qxz
+        }
+        if constexpr (kCarry || kShare4)
             dx4<N, 2, true>(sQzz + (rr + SHX) * TZ + c, TZ, a, dvx, dEr);      // duz_zdx = D+x Qzz
+        if constexpr (kShare4) {
+            c4x[0] = txr[0]; c4x[kThreads] = txr[1]; c4x[2 * kThreads] = wxr[0]; c4x[3 * kThreads] = wxr[1];
+            c4z[0] = dBr[0]; c4z[kThreads] = dBr[1]; c4z[2 * kThreads] = dEr[0]; c4z[3 * kThreads] = dEr[1];
+        }
+        if constexpr (kShare3) {
+            c3x[0] = txr[0]; c3x[kThreads] = txr[1]; c3x[2 * kThreads] = wxr[0];
+            c3z[0] = wxr[1]; c3z[kThreads] = dBr[0]; c3z[2 * kThreads] = dBr[1];
         }
         // a rolled two-iteration loop: half the code of an unrolled pair of
         // rows, which keeps the hot path inside the instruction cache
@@ -885,9 +909,15 @@ __device__ __forceinline__ bool step_tile(const StepArgs& p, const Geo& gm, cons
             const float4 opx = ldg4(p.past[0] + off + g), opz = ldg4(p.past[1] + off + g);
             const float4 osx = ldg4(p.past[2] + off + g), osz = ldg4(p.past[3] + off + g);
             float4 tx[1], wx[1], dB[1], dE[1];
-            if constexpr (kPairX) {
+            if constexpr (kCarry) {
                 tx[0] = txr[0]; wx[0] = wxr[0]; dB[0] = dBr[0]; dE[0] = dEr[0];
                 txr[0] = txr[1]; wxr[0] = wxr[1]; dBr[0] = dBr[1]; dEr[0] = dEr[1];
+            } else if constexpr (kShare4) {
+                tx[0] = c4x[q * kThreads]; wx[0] = c4x[(2 + q) * kThreads];
+                dB[0] = c4z[q * kThreads]; dE[0] = c4z[(2 + q) * kThreads];
+            } else if constexpr (kShare3) {
+                tx[0] = c3x[q * kThreads]; wx[0] = q ? c3z[0] : c3x[2 * kThreads]; dB[0] = c3z[(1 + q) * kThreads];
+                dx4<N, 1, true>(sQzz + (r + SHX) * TZ + c, TZ, a, dvx, dE);      // duz_zdx = D+x Qzz
             } else {
                 dx4<N, 1, true>(sTh + (r + SHX) * SC + scol, SC, a, dvx, tx);    // dthetadx = D+x theta
                 dx4<N, 1, false>(sOm + (r + SHX) * SC + scol, SC, a, dvx, wx);   // domegadx = D-x omega
